@@ -1,0 +1,175 @@
+/*
+ * mhd3d.h -- C-ABI of the B200 time-step library for 3dmhd.
+ *
+ * This library replaces the reference's per-step call sequence
+ *
+ *     CALL STEP            (3dmhd.f:912 -> 3dmhdsub.f:687-1176)
+ *       = CFL/Mach reduction (3dmhdsub.f:741-873)
+ *       + 3 x { FLUXES (1178-2637); RK3 axpy; BCON (2639-2958);
+ *               COMMUNICATE/COMM_MPI (2980-3141) }
+ *
+ * with one handle that keeps the prognostic state resident in GPU memory.
+ * The reference has no plugin API: STEP takes no arguments and exchanges
+ * everything through COMMON blocks (3dmhd.f:51-75).  The entry points below
+ * take those COMMON values explicitly, as plain pointers and sizes, so that
+ * a Fortran host can bind them with ISO_C_BINDING (see
+ * rast-3dmhd_b200/fortran/mhd3d_gpu.f90) and a C, C++ or Python host can
+ * bind them directly.
+ *
+ * Array conventions (all arrays are host memory, Fortran column-major):
+ *   - a 3-D field is REAL*8 (NX,NY,NZ) with NX=NPX+2, NY=NPY+2, NZ=NPZ+2,
+ *     i.e. the single-domain form of the reference's local arrays
+ *     (3dmhdparam.f:15-19 with NPEY=NPEZ=1, IX=IY=ILAP=2): one periodic
+ *     halo cell on each side in x and y, and one z ghost plane above the top
+ *     wall (K=1) and below the bottom wall (K=NZ).  The walls are the planes
+ *     K=2 and K=NZ-1.
+ *   - 1-D metric arrays have the lengths of COMMON/AJACOBI (3dmhd.f:36-38):
+ *     NX for x, NY for y, NZ for z and for RKAPA/DKAPA.
+ *
+ * Semantics follow the reference run with NPEZ>=2 (one-sided wall
+ * stencils at both walls: 3dmhdsub.f:1120-1126, 1391-1392, 1511-1513).
+ *
+ * Status codes: every entry point returns 0 on success, else one of the
+ * MHD3D_ERR_* codes.  Nothing crosses the ABI as an exception and nothing
+ * calls exit().  A handle is not thread-safe: one host thread per handle.
+ * Calls are synchronous at the ABI edge unless stated otherwise.
+ */
+#ifndef MHD3D_H
+#define MHD3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHD3D_OK               0
+#define MHD3D_ERR_ARG          1  /* bad argument or configuration the path does not support */
+#define MHD3D_ERR_CUDA         2  /* a CUDA runtime call failed */
+#define MHD3D_ERR_NONFINITE    3  /* NaN or Inf met by the CFL reduction */
+#define MHD3D_ERR_DT_SMALL     4  /* DT < 1e-8: the reference driver's emergency stop (3dmhd.f:924) */
+#define MHD3D_ERR_NO_DEVICE    5  /* no usable CUDA device */
+#define MHD3D_ERR_TIMEOUT      6  /* a bounded device-side wait gave up */
+#define MHD3D_ERR_NOMEM        7  /* device allocation failed */
+
+/* Arithmetic modes of the FP64 path. */
+#define MHD3D_MODE_EXACT 0   /* reference operation order, no FMA contraction:
+                                bit-equal to the CPU restatement (+0 == -0) */
+#define MHD3D_MODE_FAST  1   /* FMA contraction and pre-multiplied metric
+                                products; within 1e-11 of EXACT after 10 steps */
+
+/*
+ * Scalars of the COMMON blocks the step reads.  The host fills them exactly
+ * as the reference main program does (3dmhd.f:105-240), i.e. holding the
+ * float-rounded values of the REAL(4) literals (C13=1.0E00/3.0E00 etc.).
+ * They are never re-derived inside the library.
+ */
+typedef struct mhd3d_params {
+    int32_t npx, npy, npz;      /* NPX,NPY,NPZ (3dmhdparam.f:13)                 */
+    int32_t lmag, lrot;         /* LMAG, LROT (3dmhdparam.f:8)                    */
+    int32_t izcon, itcon, ibcon;/* IZC, ITC, IBC (COMMON/BCT, 3dmhdparam.f:27)   */
+    int32_t mode;               /* MHD3D_MODE_EXACT or MHD3D_MODE_FAST            */
+    int32_t reserved0;
+    /* COMMON/GRID (DD is a STEP-local scratch there and is not passed) */
+    double c13, c23, c43;
+    double hx, h2x, hy, h2y, hz, h2z;
+    /* COMMON/RUNGKU */
+    double gam1, gam2, gam3, zeta1, zeta2;
+    /* COMMON/CPAR */
+    double cv, ocv, ore, re, repr, theta, grav, gamma, sf;
+    /* COMMON/CROT */
+    double omx, omz;
+    /* COMMON/CMAG */
+    double orm, rm, obeta;
+    /* COMMON/CPEN, COMMON/CPER: bottom temperature and the upper-boundary
+       plume (used only when TP != 0 and ITC is 0 or 1, 3dmhdsub.f:2790-2826) */
+    double tb, tp, tc, xp, yp, hh;
+    /* COMMON/CTIM at the start of the run: TIMI (restart time), TIMC */
+    double timi, timc;
+    /* DT threshold of the driver's emergency stop, REAL(4) 1.0E-08 */
+    double dtmin;
+} mhd3d_params;
+
+/*
+ * Create a handle: validates the configuration, allocates the device state
+ * (U, Z and stage buffers, 1-D metrics) on the current CUDA device and
+ * copies the metric arrays.  Replaces the COMMON set-up the reference does
+ * before its main loop (3dmhd.f:105-279).
+ *
+ * Unsupported configurations return MHD3D_ERR_ARG: IXCON/IYCON != 0
+ * (FLUXES stops on those, 3dmhdsub.f:1262-1265), LREM, ID != 0, RLAX > 0,
+ * ITCON = 2 (embedded heat loss), IZCON not in {0,1}.
+ */
+int mhd3d_create(const mhd3d_params* p,
+                 const double* exx, const double* dxxdx, const double* d2xxdx2, const double* ddx,
+                 const double* wyy, const double* dyydy, const double* d2yydy2, const double* ddy,
+                 const double* zee, const double* dzzdz, const double* d2zzdz2, const double* ddz,
+                 const double* rkapa, const double* dkapa,
+                 void** handle);
+
+/* Release every device resource of the handle. */
+int mhd3d_destroy(void* handle);
+
+/*
+ * Upload the prognostic state from Fortran (NX,NY,NZ) arrays, in the order
+ * of the reference's dump records RU,RV,RW,TT,RO[,BX,BY,BZ]
+ * (3dmhd.f:941-962).  bx/by/bz may be NULL when lmag == 0.  The x/y halos
+ * of the uploaded arrays are ignored (the library wraps periodically); the
+ * z ghost planes K=1 and K=NZ are kept, as the reference keeps them.
+ */
+int mhd3d_upload(void* handle,
+                 const double* ru, const double* rv, const double* rw,
+                 const double* tt, const double* ro,
+                 const double* bx, const double* by, const double* bz);
+
+/*
+ * Download the state into Fortran (NX,NY,NZ) arrays, halos filled as
+ * COMMUNICATE leaves them (periodic copies, 3dmhdsub.f:3128-3138) and the
+ * z ghost planes as the reference leaves them.  Call before every dump.
+ */
+int mhd3d_download(void* handle,
+                   double* ru, double* rv, double* rw,
+                   double* tt, double* ro,
+                   double* bx, double* by, double* bz);
+
+/*
+ * Advance nsteps full RK3 steps: each is one CALL STEP (3dmhdsub.f:687).
+ * On return: dt = DT of the last step, timc/timt = COMMON/CTIM after it,
+ * umach = max Mach number (COMMON/TRACE), nit = COMMON/ITER NIT.
+ * Any output pointer may be NULL.  Steps stop early, with the step that
+ * produced it completed, when DT < dtmin (MHD3D_ERR_DT_SMALL, the
+ * reference's GOTO 5010 at 3dmhd.f:924) or when the CFL reduction meets
+ * a non-finite value (MHD3D_ERR_NONFINITE).
+ */
+int mhd3d_step(void* handle, int32_t nsteps,
+               double* dt, double* timc, double* timt, double* umach, int32_t* nit);
+
+/*
+ * Test-only entry points with the semantics of the Fortran routines.
+ *
+ * mhd3d_fluxes: evaluate FLUXES on the current state without changing it
+ * and copy the right-hand sides to Fortran (NX,NY,NZ) arrays: FU,FV,FW,FR,FT
+ * and, with LMAG, the induction terms WW1..WW3 (3dmhdsub.f:2129-2634).
+ * Only interior cells (I=2..NX-1, J=2..NY-1, K=2..NZ-1) are written.
+ * Values on the wall planes that BCON overwrites (FU,FV,FW,FT and WW3 at
+ * K=2 and K=NZ-1) are written as 0; the reference computes them from the
+ * ghost planes and then discards them.
+ */
+int mhd3d_fluxes(void* handle,
+                 double* fu, double* fv, double* fw, double* fr, double* ft,
+                 double* ww1, double* ww2, double* ww3);
+
+/* CFL/Mach reduction of STEP (3dmhdsub.f:741-873) on the current state. */
+int mhd3d_cfl(void* handle, double* dt, double* umach);
+
+/* BCON (3dmhdsub.f:2639-2958) applied to the current state in place. */
+int mhd3d_bcon(void* handle);
+
+/* Version string of the library. */
+const char* mhd3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHD3D_H */

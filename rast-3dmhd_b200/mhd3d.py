@@ -1,0 +1,254 @@
+"""Python binding of the 3dmhd B200 time-step library (ctypes over the C-ABI).
+
+This is the host-side mirror a Python caller uses in place of the Fortran
+driver: it builds the run set-up with libmhd3d_host.so (the driver's
+initialisation, 3dmhd.f:105-496) and drives the GPU path through
+libmhd3d_gpu.so (include/mhd3d.h), the drop-in for CALL STEP
+(3dmhd.f:912 -> 3dmhdsub.f:687).
+
+Arrays are numpy arrays in Fortran order with shape (NX, NY, NZ) =
+(NPX+2, NPY+2, NPZ+2), exactly the reference's COMMON/BIG arrays for one
+domain.  There is no CPU fallback: without the CUDA library or a GPU the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+FIELDS = ("ru", "rv", "rw", "tt", "ro", "bx", "by", "bz")
+FLUXES = ("fu", "fv", "fw", "fr", "ft", "ww1", "ww2", "ww3")
+
+MODE_EXACT = 0
+MODE_FAST = 1
+
+GRID_UNIFORM, GRID_ARCTAN, GRID_DIP, GRID_TANH_Z = 0, 1, 2, 3
+
+STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite value",
+          4: "DT below DTMIN", 5: "no CUDA device", 6: "device wait timed out", 7: "out of device memory"}
+
+
+class Mhd3dError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where}: status {code} ({STATUS.get(code, '?')})")
+        self.code = code
+
+
+class Params(C.Structure):
+    """mirror of struct mhd3d_params (include/mhd3d.h)"""
+    _fields_ = [(n, C.c_int32) for n in ("npx", "npy", "npz", "lmag", "lrot", "izcon", "itcon", "ibcon",
+                                          "mode", "reserved0")] + \
+               [(n, C.c_double) for n in ("c13", "c23", "c43", "hx", "h2x", "hy", "h2y", "hz", "h2z",
+                                           "gam1", "gam2", "gam3", "zeta1", "zeta2",
+                                           "cv", "ocv", "ore", "re", "repr", "theta", "grav", "gamma", "sf",
+                                           "omx", "omz", "orm", "rm", "obeta",
+                                           "tb", "tp", "tc", "xp", "yp", "hh", "timi", "timc", "dtmin")]
+
+
+class RunConfig(C.Structure):
+    """mirror of struct mhd3d_run_config (include/mhd3d_host.h)"""
+    _fields_ = [(n, C.c_int32) for n in ("npx", "npy", "npz", "lmag", "lrot", "izcon", "itcon", "ibcon",
+                                          "ngrid", "ntube", "seed", "mode")] + \
+               [(n, C.c_double) for n in ("xmax", "ymax", "zmax", "zstretch",
+                                           "xx1", "xx2", "yy1", "yy2", "zz1", "zz2",
+                                           "xa", "xb", "xc", "xd", "ya", "yb", "yc", "yd", "za", "zb", "zc", "zd",
+                                           "re", "pr", "theta", "grav", "ry", "ang", "rm", "beta",
+                                           "pzp", "sigma", "polys", "tp", "tc", "xp", "yp", "hh",
+                                           "ampt", "ampb", "bfh", "bzp", "zcent", "rmax", "cmt", "atube",
+                                           "gamma", "sff", "timi")]
+
+
+_DP = np.ctypeslib.ndpointer(dtype=np.float64, flags="F_CONTIGUOUS")
+_libs: dict[str, C.CDLL] = {}
+
+
+def _load(name: str) -> C.CDLL:
+    if name not in _libs:
+        path = os.path.join(HERE, name)
+        if not os.path.exists(path):
+            raise OSError(f"{path} is not built (run: make -C {HERE})")
+        _libs[name] = C.CDLL(path)
+    return _libs[name]
+
+
+def host_lib() -> C.CDLL:
+    lib = _load("libmhd3d_host.so")
+    lib.mhd3d_host_params.argtypes = [C.POINTER(RunConfig), C.POINTER(Params)]
+    lib.mhd3d_host_grid.argtypes = [C.POINTER(RunConfig)] + [C.c_void_p] * 14
+    lib.mhd3d_host_static.argtypes = [C.POINTER(RunConfig), C.c_void_p] + [C.c_void_p] * 8
+    lib.mhd3d_host_convection_config.argtypes = [C.POINTER(RunConfig), C.c_int32, C.c_int32, C.c_int32,
+                                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32]
+    lib.mhd3d_host_default_config.argtypes = [C.POINTER(RunConfig), C.c_int32, C.c_int32, C.c_int32]
+    lib.mhd3d_host_ran2.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.mhd3d_host_ran2.restype = C.c_double
+    return lib
+
+
+def gpu_lib() -> C.CDLL:
+    lib = _load("libmhd3d_gpu.so")
+    vp = C.c_void_p
+    lib.mhd3d_create.argtypes = [C.POINTER(Params)] + [vp] * 14 + [C.POINTER(vp)]
+    lib.mhd3d_destroy.argtypes = [vp]
+    lib.mhd3d_upload.argtypes = [vp] + [vp] * 8
+    lib.mhd3d_download.argtypes = [vp] + [vp] * 8
+    lib.mhd3d_step.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    lib.mhd3d_fluxes.argtypes = [vp] + [vp] * 8
+    lib.mhd3d_cfl.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.mhd3d_bcon.argtypes = [vp]
+    lib.mhd3d_version.restype = C.c_char_p
+    return lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+GRID_NAMES = ("exx", "dxxdx", "d2xxdx2", "ddx", "wyy", "dyydy", "d2yydy2", "ddy",
+              "zee", "dzzdz", "d2zzdz2", "ddz", "rkapa", "dkapa")
+
+
+@dataclass
+class Setup:
+    """Everything the driver holds before its first CALL STEP."""
+    config: RunConfig
+    params: Params
+    grid: dict
+    state: dict
+
+    @property
+    def shape(self):
+        p = self.params
+        return (p.npx + 2, p.npy + 2, p.npz + 2)
+
+    def grid_args(self):
+        return [_ptr(self.grid[n]) for n in GRID_NAMES]
+
+    def copy_state(self) -> dict:
+        return {k: (None if v is None else v.copy(order="F")) for k, v in self.state.items()}
+
+
+def default_config(npx: int, npy: int, npz: int) -> RunConfig:
+    c = RunConfig()
+    host_lib().mhd3d_host_default_config(C.byref(c), npx, npy, npz)
+    return c
+
+
+def convection_config(npx: int, npy: int, npz: int, ra: float = 1e5, ta: float = 1e4, pr: float = 1.0,
+                      pm: float = 4.0, contrast: float = 10.0, m: float = 1.0, beta: float = 1e4,
+                      stretch: float = 1.5, ampt: float = 2e-4, seed: int = 62659) -> RunConfig:
+    """Rotating MHD polytrope from dimensionless numbers (mid-depth convention)."""
+    c = RunConfig()
+    host_lib().mhd3d_host_convection_config(C.byref(c), npx, npy, npz, ra, ta, pr, pm, contrast, m, beta,
+                                            stretch, ampt, seed)
+    return c
+
+
+def make_setup(cfg: RunConfig) -> Setup:
+    lib = host_lib()
+    p = Params()
+    st = lib.mhd3d_host_params(C.byref(cfg), C.byref(p))
+    if st:
+        raise Mhd3dError(st, "mhd3d_host_params")
+    nx, ny, nz = cfg.npx + 2, cfg.npy + 2, cfg.npz + 2
+    lens = (nx,) * 4 + (ny,) * 4 + (nz,) * 6
+    grid = {n: np.zeros(L) for n, L in zip(GRID_NAMES, lens)}
+    st = lib.mhd3d_host_grid(C.byref(cfg), *[_ptr(grid[n]) for n in GRID_NAMES])
+    if st:
+        raise Mhd3dError(st, "mhd3d_host_grid")
+    shape = (nx, ny, nz)
+    state = {f: np.zeros(shape, order="F") for f in FIELDS[:5]}
+    for f in FIELDS[5:]:
+        state[f] = np.zeros(shape, order="F") if cfg.lmag else None
+    st = lib.mhd3d_host_static(C.byref(cfg), _ptr(grid["zee"]), *[_ptr(state[f]) for f in FIELDS])
+    if st:
+        raise Mhd3dError(st, "mhd3d_host_static")
+    return Setup(cfg, p, grid, state)
+
+
+def wrap_periodic(a: np.ndarray) -> np.ndarray:
+    """COMM_MPI's periodic copies (y then x) on a Fortran (NX,NY,NZ) array, in place."""
+    a[:, 0, :] = a[:, -2, :]
+    a[:, -1, :] = a[:, 1, :]
+    a[0, :, :] = a[-2, :, :]
+    a[-1, :, :] = a[1, :, :]
+    return a
+
+
+class GpuSim:
+    """A handle of the GPU time-step library (one per simulation)."""
+
+    def __init__(self, setup: Setup, mode: int | None = None):
+        self.lib = gpu_lib()
+        self.setup = setup
+        p = Params.from_buffer_copy(setup.params)
+        if mode is not None:
+            p.mode = mode
+        self.params = p
+        self.h = C.c_void_p()
+        st = self.lib.mhd3d_create(C.byref(p), *setup.grid_args(), C.byref(self.h))
+        if st:
+            raise Mhd3dError(st, "mhd3d_create")
+
+    def close(self):
+        if self.h:
+            self.lib.mhd3d_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, state: dict):
+        st = self.lib.mhd3d_upload(self.h, *[_ptr(state.get(f)) for f in FIELDS])
+        if st:
+            raise Mhd3dError(st, "mhd3d_upload")
+
+    def download(self) -> dict:
+        shape = self.setup.shape
+        lmag = self.params.lmag
+        out = {f: np.zeros(shape, order="F") for f in FIELDS[:5]}
+        for f in FIELDS[5:]:
+            out[f] = np.zeros(shape, order="F") if lmag else None
+        st = self.lib.mhd3d_download(self.h, *[_ptr(out[f]) for f in FIELDS])
+        if st:
+            raise Mhd3dError(st, "mhd3d_download")
+        return out
+
+    def step(self, n: int = 1, check: bool = True) -> dict:
+        dt, timc, timt, umach = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        nit = C.c_int32()
+        st = self.lib.mhd3d_step(self.h, n, C.byref(dt), C.byref(timc), C.byref(timt), C.byref(umach),
+                                 C.byref(nit))
+        if st and check:
+            raise Mhd3dError(st, "mhd3d_step")
+        return {"status": st, "dt": dt.value, "timc": timc.value, "timt": timt.value,
+                "umach": umach.value, "nit": nit.value}
+
+    def fluxes(self) -> dict:
+        shape = self.setup.shape
+        out = {f: np.zeros(shape, order="F") for f in FLUXES}
+        st = self.lib.mhd3d_fluxes(self.h, *[_ptr(out[f]) for f in FLUXES])
+        if st:
+            raise Mhd3dError(st, "mhd3d_fluxes")
+        return out
+
+    def cfl(self):
+        dt, um = C.c_double(), C.c_double()
+        st = self.lib.mhd3d_cfl(self.h, C.byref(dt), C.byref(um))
+        if st:
+            raise Mhd3dError(st, "mhd3d_cfl")
+        return dt.value, um.value
+
+    def bcon(self):
+        st = self.lib.mhd3d_bcon(self.h)
+        if st:
+            raise Mhd3dError(st, "mhd3d_bcon")
