@@ -1,0 +1,539 @@
+// mhd3d_api.cu -- the C-ABI of include/mhd3d.h: handle life cycle, layout
+// conversion between the reference's Fortran arrays and the device layout,
+// and the step loop with its device-side bookkeeping.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "../../include/mhd3d.h"
+#include "mhd3d_dev.cuh"
+
+namespace mhd3d {
+namespace {
+
+struct Handle {
+    mhd3d_params p;
+    int dev = -1;
+    cudaStream_t st = nullptr;
+    int nf = 0, pitch = 0;
+    size_t pstride = 0, fstride = 0;
+    double* ubuf[2] = {nullptr, nullptr};
+    int cur = 0;               // ubuf[cur] holds the current state
+    double* z = nullptr;
+    double* ghost = nullptr;
+    double* gro = nullptr;
+    double* stage = nullptr;   // one Fortran (NX,NY,NZ) field
+    double* fout = nullptr;
+    double* met = nullptr;     // all 1-D arrays, packed
+    Control* ctl = nullptr;
+    Accum* acc = nullptr;
+    Metrics m{};
+    Scalars s{};
+    int ntx = 0, zlen = 0, nchunks = 0;
+    bool dt_valid = false;
+    int gparity = 0;           // host copy of Control::gparity
+};
+
+#define CK(x)                                                                                    \
+    do {                                                                                         \
+        cudaError_t e_ = (x);                                                                    \
+        if (e_ != cudaSuccess) {                                                                 \
+            std::fprintf(stderr, "mhd3d: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_),   \
+                         __FILE__, __LINE__);                                                     \
+            return e_ == cudaErrorMemoryAllocation ? MHD3D_ERR_NOMEM : MHD3D_ERR_CUDA;            \
+        }                                                                                        \
+    } while (0)
+
+__global__ void k_unpack(const double* __restrict__ fort, double* __restrict__ u, double* __restrict__ g,
+                         int npx, int npy, int npz, int pitch, size_t pstride)
+{
+    // Fortran (NX,NY,NZ) -> interior planes of u and the two ghost planes of g
+    const int NX = npx + 2, NY = npy + 2;
+    const size_t n = (size_t)npx * npy * (npz + 2);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % npx), j = (int)((q / npx) % npy), K = (int)(q / ((size_t)npx * npy));
+        const double v = fort[(size_t)(i + 1) + (size_t)NX * ((size_t)(j + 1) + (size_t)NY * K)];
+        if (K == 0) g[(size_t)j * pitch + i] = v;
+        else if (K == npz + 1) g[(size_t)npy * pitch + (size_t)j * pitch + i] = v;
+        else u[(size_t)(K - 1) * pstride + (size_t)j * pitch + i] = v;
+    }
+}
+
+__global__ void k_pack(const double* __restrict__ u, const double* __restrict__ g, double* __restrict__ fort,
+                       int npx, int npy, int npz, int pitch, size_t pstride, int interior_only)
+{
+    // device layout -> Fortran (NX,NY,NZ) with the periodic halos COMMUNICATE leaves
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        if (interior_only) {
+            if (I == 0 || I == NX - 1 || J == 0 || J == NY - 1 || K == 0 || K == NZ - 1) {
+                fort[q] = 0.0;
+                continue;
+            }
+        }
+        int i = I - 1, j = J - 1;
+        i = i < 0 ? i + npx : (i >= npx ? i - npx : i);
+        j = j < 0 ? j + npy : (j >= npy ? j - npy : j);
+        double v;
+        if (K == 0) v = g[(size_t)j * pitch + i];
+        else if (K == NZ - 1) v = g[(size_t)npy * pitch + (size_t)j * pitch + i];
+        else v = u[(size_t)(K - 1) * pstride + (size_t)j * pitch + i];
+        fort[q] = v;
+    }
+}
+
+__global__ void k_reset(Control* ctl, Accum* acc, int clear_stop)
+{
+    for (int i = 0; i < 4; ++i) acc->wmin[i] = ~0ull;
+    acc->umax = 0ull;
+    acc->bad = 0u;
+    if (clear_stop) {
+        ctl->stop = 0;
+        ctl->status = 0;
+    }
+}
+
+// End of a step (advance=1: NIT, TIMC, TIMT of STEP 3dmhdsub.f:1171-1173 and
+// the driver's DT check 3dmhd.f:924) and DT/UMACH of the next step from the
+// CFL accumulators (DT=SF*MIN(...), 3dmhdsub.f:866-873; UMACH=SQRT(...), 761).
+__global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance)
+{
+    if (advance) {
+        if (ctl->stop) return;
+        ctl->timc = ctl->timc + ctl->dt;
+        ctl->timt = ctl->timi + ctl->timc;
+        ctl->nit += 1;
+        ctl->last_dt = ctl->dt;
+        ctl->last_umach = ctl->umach;
+        ctl->gparity ^= 1;
+        if (!(ctl->dt >= dtmin)) {
+            ctl->stop = 1;
+            ctl->status = isfinite(ctl->dt) ? MHD3D_ERR_DT_SMALL : MHD3D_ERR_NONFINITE;
+        }
+    }
+    double w = of_key(acc->wmin[0]);
+    const double w2 = of_key(acc->wmin[1]), w3 = of_key(acc->wmin[2]), w4 = of_key(acc->wmin[3]);
+    w = w2 < w ? w2 : w;
+    w = w3 < w ? w3 : w;
+    if (lmag) w = w4 < w ? w4 : w;
+    ctl->dt = sf * w;
+    ctl->umach = sqrt(of_key(acc->umax));
+    if (acc->bad && !ctl->stop) {
+        ctl->stop = 1;
+        ctl->status = MHD3D_ERR_NONFINITE;
+    }
+    for (int i = 0; i < 4; ++i) acc->wmin[i] = ~0ull;
+    acc->umax = 0ull;
+    acc->bad = 0u;
+}
+
+unsigned grid_for(size_t n)
+{
+    size_t b = (n + 255) / 256;
+    return (unsigned)(b > 148 * 16 ? 148 * 16 : (b ? b : 1));
+}
+
+StageArgs make_args(Handle* h)
+{
+    StageArgs a{};
+    a.u_in = h->ubuf[h->cur];
+    a.u_out = h->ubuf[h->cur ^ 1];
+    a.z = h->z;
+    a.f_out = h->fout;
+    a.ghost = h->ghost;
+    a.gro = h->gro;
+    a.ctl = h->ctl;
+    a.acc = h->acc;
+    a.m = h->m;
+    a.s = h->s;
+    a.fstride = h->fstride;
+    a.pstride = h->pstride;
+    a.ntx = h->ntx;
+    a.zlen = h->zlen;
+    a.nchunks = h->nchunks;
+    return a;
+}
+
+cudaError_t launch_stage(Handle* h, int stage, const StageArgs& a)
+{
+    return h->p.mode == MHD3D_MODE_FAST ? fast::launch_stage(stage, a, h->st) : exact::launch_stage(stage, a, h->st);
+}
+
+cudaError_t launch_cfl(Handle* h, const StageArgs& a)
+{
+    return h->p.mode == MHD3D_MODE_FAST ? fast::launch_cfl(a, h->st) : exact::launch_cfl(a, h->st);
+}
+
+int validate(const mhd3d_params* p)
+{
+    if (!p) return MHD3D_ERR_ARG;
+    if (p->npx < 2 || p->npy < 2 || p->npz < 4) return MHD3D_ERR_ARG;
+    if (p->izcon != 0 && p->izcon != 1) return MHD3D_ERR_ARG;
+    if (p->itcon < 0 || p->itcon > 4 || p->itcon == 2) return MHD3D_ERR_ARG;
+    if (p->mode != MHD3D_MODE_EXACT && p->mode != MHD3D_MODE_FAST) return MHD3D_ERR_ARG;
+    if ((size_t)(p->npx + 2) * (p->npy + 2) * (p->npz + 2) > ((size_t)1 << 40)) return MHD3D_ERR_ARG;
+    return MHD3D_OK;
+}
+
+int destroy(Handle* h)
+{
+    if (!h) return MHD3D_OK;
+    if (h->dev >= 0) cudaSetDevice(h->dev);
+    cudaFree(h->ubuf[0]);
+    cudaFree(h->ubuf[1]);
+    cudaFree(h->z);
+    cudaFree(h->ghost);
+    cudaFree(h->gro);
+    cudaFree(h->stage);
+    cudaFree(h->fout);
+    cudaFree(h->met);
+    cudaFree(h->ctl);
+    cudaFree(h->acc);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return MHD3D_OK;
+}
+
+int create(const mhd3d_params* p, const double* const arrs[14], void** out)
+{
+    int st = validate(p);
+    if (st) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MHD3D_ERR_NO_DEVICE;
+    for (int i = 0; i < 14; ++i)
+        if (!arrs[i]) return MHD3D_ERR_ARG;
+    Handle* h = new (std::nothrow) Handle();
+    if (!h) return MHD3D_ERR_NOMEM;
+    *out = h;   // released by the caller if anything below fails
+    h->p = *p;
+    CK(cudaGetDevice(&h->dev));
+    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    const int npx = p->npx, npy = p->npy, npz = p->npz;
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    h->nf = p->lmag ? 8 : 5;
+    h->pitch = (npx + 31) / 32 * 32;
+    h->pstride = (size_t)npy * h->pitch;
+    h->fstride = (size_t)npz * h->pstride;
+    const size_t ubytes = sizeof(double) * h->nf * h->fstride;
+    CK(cudaMalloc(&h->ubuf[0], ubytes));
+    CK(cudaMalloc(&h->ubuf[1], ubytes));
+    CK(cudaMalloc(&h->z, ubytes));
+    CK(cudaMemset(h->ubuf[0], 0, ubytes));
+    CK(cudaMemset(h->ubuf[1], 0, ubytes));
+    CK(cudaMemset(h->z, 0, ubytes));
+    const size_t gplane = (size_t)npy * h->pitch;
+    CK(cudaMalloc(&h->ghost, sizeof(double) * 8 * 2 * gplane));
+    CK(cudaMemset(h->ghost, 0, sizeof(double) * 8 * 2 * gplane));
+    CK(cudaMalloc(&h->gro, sizeof(double) * 2 * 2 * gplane));
+    CK(cudaMemset(h->gro, 0, sizeof(double) * 2 * 2 * gplane));
+    CK(cudaMalloc(&h->stage, sizeof(double) * (size_t)NX * NY * NZ));
+    CK(cudaMalloc(&h->ctl, sizeof(Control)));
+    CK(cudaMalloc(&h->acc, sizeof(Accum)));
+
+    // 1-D arrays: 11 metric/kappa arrays and the two plume factors
+    const int lens[13] = {NX, NX, NX, NY, NY, NY, NZ, NZ, NZ, NZ, NZ, NX, NY};
+    size_t tot = 0;
+    for (int i = 0; i < 13; ++i) tot += lens[i];
+    double* hm = (double*)std::malloc(sizeof(double) * tot);
+    const double* exx = arrs[0];
+    const double* wyy = arrs[4];
+    const double* src[11] = {arrs[1], arrs[2], arrs[3], arrs[5], arrs[6], arrs[7], arrs[9], arrs[10], arrs[11],
+                             arrs[12], arrs[13]};
+    size_t off = 0;
+    size_t offs[13];
+    for (int i = 0; i < 11; ++i) {
+        offs[i] = off;
+        std::memcpy(hm + off, src[i], sizeof(double) * lens[i]);
+        off += lens[i];
+    }
+    // plume factors EXP(CLN*(EXX(I)-XP)**2), EXP(CLN*(WYY(J)-YP)**2) with
+    // CLN=-4.0E00*LOG(2.0E00)/HH/HH (3dmhdsub.f:2818, 2803-2804)
+    const int plume = (p->tp != 0.0 && (p->itcon == 0 || p->itcon == 1)) ? 1 : 0;
+    const double cln = plume ? (double)(-(4.0f * std::log(2.0f))) / p->hh / p->hh : 0.0;
+    offs[11] = off;
+    for (int i = 0; i < NX; ++i) {
+        const double d = exx[i] - p->xp;
+        hm[off + i] = plume ? std::exp(cln * (d * d)) : 0.0;
+    }
+    off += NX;
+    offs[12] = off;
+    for (int j = 0; j < NY; ++j) {
+        const double d = wyy[j] - p->yp;
+        hm[off + j] = plume ? std::exp(cln * (d * d)) : 0.0;
+    }
+    off += NY;
+    CK(cudaMalloc(&h->met, sizeof(double) * tot));
+    CK(cudaMemcpy(h->met, hm, sizeof(double) * tot, cudaMemcpyHostToDevice));
+    h->m.dxxdx = h->met + offs[0];
+    h->m.d2xxdx2 = h->met + offs[1];
+    h->m.ddx = h->met + offs[2];
+    h->m.dyydy = h->met + offs[3];
+    h->m.d2yydy2 = h->met + offs[4];
+    h->m.ddy = h->met + offs[5];
+    h->m.dzzdz = h->met + offs[6];
+    h->m.d2zzdz2 = h->met + offs[7];
+    h->m.ddz = h->met + offs[8];
+    h->m.rkapa = h->met + offs[9];
+    h->m.dkapa = h->met + offs[10];
+    h->m.plume_gx = h->met + offs[11];
+    h->m.plume_gy = h->met + offs[12];
+
+    // scalars (3dmhd.f:105-240 values; FLUXES/BCON per-call products)
+    Scalars& s = h->s;
+    s.c13 = p->c13; s.c23 = p->c23; s.c43 = p->c43;
+    s.hx = p->hx; s.h2x = p->h2x; s.hy = p->hy; s.h2y = p->h2y; s.hz = p->hz; s.h2z = p->h2z;
+    s.gam1 = p->gam1; s.gam2 = p->gam2; s.gam3 = p->gam3; s.zeta1 = p->zeta1; s.zeta2 = p->zeta2;
+    s.cv = p->cv; s.ocv = p->ocv; s.ore = p->ore; s.re = p->re; s.repr = p->repr;
+    s.theta = p->theta; s.grav = p->grav; s.gamma = p->gamma; s.ogamma = 1.0 / p->gamma; s.sf = p->sf;
+    s.rm = p->rm; s.omx = p->omx; s.omz = p->omz; s.orm = p->orm; s.obeta = p->obeta;
+    s.tmp_cond = p->ocv / p->repr;
+    s.tmp_a = p->ocv * p->ore;
+    s.tmp_b = p->c43 * p->ocv * p->ore;
+    s.tmp_13 = p->c13 * p->ore;
+    s.tmp_m = p->obeta * p->orm * p->ocv;
+    s.tb = p->tb; s.tp = p->tp; s.tc = p->tc; s.hh = p->hh;
+    const double dzs = (double)(1.0f / (float)(npz - 1));
+    s.top_dz = dzs / src[6][1];                         // DZ=1.0E00/FLOAT(NPZ-1)/DZZDZ(2)
+    s.top_flux = p->c23 * s.top_dz * p->theta;
+    const double bot_dz = dzs / src[6][NZ - 2];         // DZZDZ(NZ-1)
+    s.bot_flux = p->c23 * bot_dz * p->theta / src[9][NZ - 2];
+    s.dtmin = p->dtmin;
+    s.timi = p->timi;
+    s.npx = npx; s.npy = npy; s.npz = npz; s.pitch = h->pitch;
+    s.lmag = p->lmag; s.lrot = p->lrot; s.izcon = p->izcon; s.itcon = p->itcon; s.ibcon = p->ibcon;
+    s.plume = plume;
+    std::free(hm);
+
+    // work decomposition: TX x TY tiles, z chunks of >= 3 planes
+    h->ntx = (npx + TX - 1) / TX;
+    const int target = 64;
+    int nch = (npz + target - 1) / target;
+    while (nch > 1 && npz / nch < 3) --nch;
+    h->nchunks = nch;
+    h->zlen = npz / nch;
+
+    Control c0{};
+    c0.timc = p->timc;
+    c0.timi = p->timi;
+    c0.timt = 0.0;
+    CK(cudaMemcpy(h->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice));
+    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    *out = h;
+    return MHD3D_OK;
+}
+
+int upload(Handle* h, const double* const f[8])
+{
+    CK(cudaSetDevice(h->dev));
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
+    const size_t gplane = (size_t)npy * h->pitch;
+    for (int i = 0; i < h->nf; ++i)
+        if (!f[i]) return MHD3D_ERR_ARG;
+    for (int fi = 0; fi < h->nf; ++fi) {
+        CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyHostToDevice, h->st));
+        double* g = (fi == F_RO) ? h->gro : h->ghost + (size_t)fi * 2 * gplane;
+        k_unpack<<<grid_for((size_t)npx * npy * (npz + 2)), 256, 0, h->st>>>(
+            h->stage, h->ubuf[h->cur] + (size_t)fi * h->fstride, g, npx, npy, npz, h->pitch, h->pstride);
+        CK(cudaGetLastError());
+    }
+    // the uploaded RO ghost planes are the current copy
+    Control c{};
+    CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    c.gparity = 0;
+    h->gparity = 0;
+    CK(cudaMemcpyAsync(h->ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->dt_valid = false;
+    return MHD3D_OK;
+}
+
+int download(Handle* h, double* const f[8])
+{
+    CK(cudaSetDevice(h->dev));
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
+    const size_t gplane = (size_t)npy * h->pitch;
+    for (int fi = 0; fi < h->nf; ++fi) {
+        if (!f[fi]) continue;
+        const double* g = (fi == F_RO) ? h->gro + (size_t)h->gparity * 2 * gplane : h->ghost + (size_t)fi * 2 * gplane;
+        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->fstride, g, h->stage, npx, npy,
+                                                    npz, h->pitch, h->pstride, 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
+int initial_dt(Handle* h)
+{
+    StageArgs a = make_args(h);
+    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+    CK(cudaGetLastError());
+    CK(launch_cfl(h, a));
+    k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 0);
+    CK(cudaGetLastError());
+    h->dt_valid = true;
+    return MHD3D_OK;
+}
+
+int step(Handle* h, int n, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
+{
+    CK(cudaSetDevice(h->dev));
+    if (n < 0) return MHD3D_ERR_ARG;
+    Control c0{};
+    CK(cudaMemcpyAsync(&c0, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    // every call starts with a clear stop flag; DT of the current state comes
+    // from the last stage-3 reduction, or from a fresh CFL pass after a change
+    if (!h->dt_valid) {
+        int st = initial_dt(h);
+        if (st) return st;
+    } else {
+        k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+        CK(cudaGetLastError());
+    }
+    const int cur0 = h->cur;
+    int cur = cur0;
+    for (int s = 0; s < n; ++s) {
+        for (int stg = 1; stg <= 3; ++stg) {
+            StageArgs a = make_args(h);
+            a.u_in = h->ubuf[cur];
+            a.u_out = h->ubuf[cur ^ 1];
+            CK(launch_stage(h, stg, a));
+            cur ^= 1;
+        }
+        k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 1);
+        CK(cudaGetLastError());
+    }
+    Control c{};
+    CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const int ran = c.nit - c0.nit;
+    h->cur = cur0 ^ (ran & 1);
+    h->gparity = c.gparity;
+    if (dt) *dt = c.last_dt;
+    if (timc) *timc = c.timc;
+    if (timt) *timt = c.timt;
+    if (umach) *umach = c.last_umach;
+    if (nit) *nit = c.nit;
+    return c.stop ? c.status : MHD3D_OK;
+}
+
+int fluxes(Handle* h, double* const out[8])
+{
+    CK(cudaSetDevice(h->dev));
+    if (!h->fout) CK(cudaMalloc(&h->fout, sizeof(double) * h->nf * h->fstride));
+    StageArgs a = make_args(h);
+    CK(launch_stage(h, 0, a));
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
+    for (int fi = 0; fi < h->nf; ++fi) {
+        if (!out[fi]) continue;
+        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->fout + (size_t)fi * h->fstride, h->ghost, h->stage, npx, npy,
+                                                    npz, h->pitch, h->pstride, 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
+}  // namespace
+}  // namespace mhd3d
+
+using namespace mhd3d;
+
+extern "C" {
+
+int mhd3d_create(const mhd3d_params* p,
+                 const double* exx, const double* dxxdx, const double* d2xxdx2, const double* ddx,
+                 const double* wyy, const double* dyydy, const double* d2yydy2, const double* ddy,
+                 const double* zee, const double* dzzdz, const double* d2zzdz2, const double* ddz,
+                 const double* rkapa, const double* dkapa, void** handle)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    *handle = nullptr;
+    const double* arrs[14] = {exx, dxxdx, d2xxdx2, ddx, wyy, dyydy, d2yydy2, ddy, zee, dzzdz, d2zzdz2, ddz, rkapa, dkapa};
+    void* h = nullptr;
+    int st = create(p, arrs, &h);
+    if (st) {
+        destroy(static_cast<Handle*>(h));
+        return st;
+    }
+    *handle = h;
+    return MHD3D_OK;
+}
+
+int mhd3d_destroy(void* handle) { return destroy(static_cast<Handle*>(handle)); }
+
+int mhd3d_upload(void* handle, const double* ru, const double* rv, const double* rw, const double* tt,
+                 const double* ro, const double* bx, const double* by, const double* bz)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    const double* f[8] = {ru, rv, rw, tt, ro, bx, by, bz};
+    return upload(static_cast<Handle*>(handle), f);
+}
+
+int mhd3d_download(void* handle, double* ru, double* rv, double* rw, double* tt, double* ro, double* bx,
+                   double* by, double* bz)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    double* f[8] = {ru, rv, rw, tt, ro, bx, by, bz};
+    return download(static_cast<Handle*>(handle), f);
+}
+
+int mhd3d_step(void* handle, int32_t nsteps, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    return step(static_cast<Handle*>(handle), nsteps, dt, timc, timt, umach, nit);
+}
+
+int mhd3d_fluxes(void* handle, double* fu, double* fv, double* fw, double* fr, double* ft, double* ww1,
+                 double* ww2, double* ww3)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    double* o[8] = {fu, fv, fw, fr, ft, ww1, ww2, ww3};
+    return fluxes(static_cast<Handle*>(handle), o);
+}
+
+int mhd3d_cfl(void* handle, double* dt, double* umach)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    Handle* h = static_cast<Handle*>(handle);
+    CK(cudaSetDevice(h->dev));
+    int st = initial_dt(h);
+    if (st) return st;
+    Control c{};
+    CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (dt) *dt = c.dt;
+    if (umach) *umach = c.umach;
+    return c.stop ? c.status : MHD3D_OK;
+}
+
+int mhd3d_bcon(void* handle)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    Handle* h = static_cast<Handle*>(handle);
+    CK(cudaSetDevice(h->dev));
+    StageArgs a = make_args(h);
+    CK(h->p.mode == MHD3D_MODE_FAST ? fast::launch_bcon(a, h->st) : exact::launch_bcon(a, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->dt_valid = false;
+    return MHD3D_OK;
+}
+
+const char* mhd3d_version(void) { return "mhd3d-b200 0.1 (sm_100a, FP64)"; }
+
+}  // extern "C"

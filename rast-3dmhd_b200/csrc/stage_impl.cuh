@@ -1,0 +1,732 @@
+// stage_impl.cuh -- the fused RK3 stage kernel (RHS + update + BCON +
+// ghost-plane toggle + CFL reduction) and the standalone CFL/BCON kernels.
+//
+// Included twice: by stage_exact.cu (compiled with -fmad=false, so every
+// product and sum is rounded separately, as gfortran -O2 evaluates the
+// reference) and by stage_fast.cu (FMA contraction allowed).  MHD3D_NS names
+// the namespace of each copy.
+//
+// Work decomposition: a CTA owns a TX x TY tile of (x,y) columns and a
+// chunk of z planes and marches down the chunk.  Planes k-1, k, k+1 of the
+// prognostic fields plus the quantities FLUXES derives on the whole array
+// (1/RO, UU,VV,WW, pressure) sit in a 3-slot shared-memory ring with a
+// one-cell periodic halo, so every right-hand-side term of FLUXES
+// (3dmhdsub.f:1249-2634), including the 19-point cross terms of the
+// viscous stress, reads shared memory only.  The wall planes take BCON
+// (2751-2955) in the same pass: the thread owning a column keeps the new
+// values of the two planes next to each wall in registers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/mhd3d.h"
+#include "mhd3d_dev.cuh"
+
+namespace mhd3d {
+namespace MHD3D_NS {
+
+template <bool MAG>
+struct NQ_ {
+    static constexpr int value = MAG ? 13 : 10;
+};
+// shared-memory quantity slots
+enum Q { Q_RU = 0, Q_RV, Q_RW, Q_RO, Q_TT, Q_RI, Q_UU, Q_VV, Q_WW, Q_P, Q_BX, Q_BY, Q_BZ };
+
+__device__ __forceinline__ int wrapi(int v, int n)
+{
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+
+// Load plane kp (-1 and npz are the ghost planes) of the tile into ring slot.
+template <bool MAG>
+__device__ __forceinline__ void load_plane(const StageArgs& a, double* __restrict__ sm, int slot, int kp,
+                                           int x0, int y0, int rd)
+{
+    constexpr int NQ = NQ_<MAG>::value;
+    const int npx = a.s.npx, npy = a.s.npy, npz = a.s.npz, pitch = a.s.pitch;
+    double* base = sm + (size_t)slot * NQ * SX * SY;
+    for (int p = threadIdx.x; p < SX * SY; p += NT) {
+        const int lx = p % SX, ly = p / SX;
+        const int gx = wrapi(x0 - 1 + lx, npx), gy = wrapi(y0 - 1 + ly, npy);
+        double ru, rv, rw, ro, tt, bx = 0, by = 0, bz = 0;
+        if (kp >= 0 && kp < npz) {
+            const size_t c = (size_t)kp * a.pstride + (size_t)gy * pitch + gx;
+            ru = a.u_in[c + F_RU * a.fstride];
+            rv = a.u_in[c + F_RV * a.fstride];
+            rw = a.u_in[c + F_RW * a.fstride];
+            tt = a.u_in[c + F_TT * a.fstride];
+            ro = a.u_in[c + F_RO * a.fstride];
+            if (MAG) {
+                bx = a.u_in[c + F_BX * a.fstride];
+                by = a.u_in[c + F_BY * a.fstride];
+                bz = a.u_in[c + F_BZ * a.fstride];
+            }
+        } else {
+            const int g = kp < 0 ? 0 : 1;
+            const size_t gp = (size_t)npy * pitch;
+            const size_t c = (size_t)g * gp + (size_t)gy * pitch + gx;
+            ru = a.ghost[(size_t)F_RU * 2 * gp + c];
+            rv = a.ghost[(size_t)F_RV * 2 * gp + c];
+            rw = a.ghost[(size_t)F_RW * 2 * gp + c];
+            tt = a.ghost[(size_t)F_TT * 2 * gp + c];
+            ro = a.gro[(size_t)rd * 2 * gp + c];
+            if (MAG) {
+                bx = a.ghost[(size_t)F_BX * 2 * gp + c];
+                by = a.ghost[(size_t)F_BY * 2 * gp + c];
+                bz = a.ghost[(size_t)F_BZ * 2 * gp + c];
+            }
+        }
+        // loops 90 and 160-180 of FLUXES: pressure from rho, then 1/rho and u=rho*u*(1/rho)
+        const double pr = ro * tt;
+        const double ri = 1.0 / ro;
+        double* q = base + ly * SX + lx;
+        q[Q_RU * SX * SY] = ru;
+        q[Q_RV * SX * SY] = rv;
+        q[Q_RW * SX * SY] = rw;
+        q[Q_RO * SX * SY] = ro;
+        q[Q_TT * SX * SY] = tt;
+        q[Q_RI * SX * SY] = ri;
+        q[Q_UU * SX * SY] = ru * ri;
+        q[Q_VV * SX * SY] = rv * ri;
+        q[Q_WW * SX * SY] = rw * ri;
+        q[Q_P * SX * SY] = pr;
+        if (MAG) {
+            q[Q_BX * SX * SY] = bx;
+            q[Q_BY * SX * SY] = by;
+            q[Q_BZ * SX * SY] = bz;
+        }
+    }
+}
+
+// CFL limits of one cell (STEP loops 10-50 and 2, 3dmhdsub.f:749-857).
+struct CflPart {
+    double w1, w2, w3, w4, mach2;
+    bool bad;
+};
+
+template <bool MAG>
+__device__ __forceinline__ void cfl_cell(const Scalars& s, double ru, double rv, double rw, double ro, double tt,
+                                         double bx, double by, double bz, double dd, double rkapa, CflPart& c)
+{
+    const double r = 1.0 / ro;
+    const double uu = (ru * ru + rv * rv + rw * rw) * (r * r);
+    c.mach2 = s.ogamma * uu / tt;
+    double fast2;
+    if (MAG) {
+        const double b2o = (bx * bx + by * by + bz * bz) * s.obeta / ro;
+        fast2 = uu + s.gamma * tt + b2o + 2.0 * sqrt(uu * (s.gamma * tt + b2o));
+    } else {
+        fast2 = uu + s.gamma * tt + 2.0 * sqrt(uu * s.gamma * tt);
+    }
+    c.w1 = dd / sqrt(fast2);
+    c.w2 = 0.5 * dd * dd * s.repr * s.cv * ro / rkapa;
+    c.w3 = 0.375 * dd * dd * s.re * ro;
+    c.w4 = MAG ? 0.5 * dd * dd * s.rm : 0.0;
+    c.bad = !(isfinite(c.w1) && isfinite(c.w2) && isfinite(c.w3) && isfinite(c.mach2));
+}
+
+__device__ __forceinline__ double cell_dd(const Metrics& m, int gi, int gj, int k)
+{
+    // DD=MIN(DDX(I),DDY(J),DDZ(K))
+    return dmin(dmin(m.ddx[gi + 1], m.ddy[gj + 1]), m.ddz[k + 1]);
+}
+
+// Block-wide reduction of the CFL parts into the global accumulators.
+__device__ __forceinline__ void cfl_commit(Accum* acc, unsigned long long k1, unsigned long long k2,
+                                           unsigned long long k3, unsigned long long k4, unsigned long long km,
+                                           unsigned int bad, unsigned long long* red)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        k1 = min(k1, __shfl_xor_sync(0xffffffffu, k1, o));
+        k2 = min(k2, __shfl_xor_sync(0xffffffffu, k2, o));
+        k3 = min(k3, __shfl_xor_sync(0xffffffffu, k3, o));
+        k4 = min(k4, __shfl_xor_sync(0xffffffffu, k4, o));
+        km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        red[w * 6 + 0] = k1;
+        red[w * 6 + 1] = k2;
+        red[w * 6 + 2] = k3;
+        red[w * 6 + 3] = k4;
+        red[w * 6 + 4] = km;
+        red[w * 6 + 5] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < NT / 32; ++i) {
+            k1 = min(k1, red[i * 6 + 0]);
+            k2 = min(k2, red[i * 6 + 1]);
+            k3 = min(k3, red[i * 6 + 2]);
+            k4 = min(k4, red[i * 6 + 3]);
+            km = max(km, red[i * 6 + 4]);
+            bad |= (unsigned int)red[i * 6 + 5];
+        }
+        atomicMin(&acc->wmin[0], k1);
+        atomicMin(&acc->wmin[1], k2);
+        atomicMin(&acc->wmin[2], k3);
+        atomicMin(&acc->wmin[3], k4);
+        atomicMax(&acc->umax, km);
+        if (bad) atomicOr(&acc->bad, 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The stage kernel.  STAGE 0: right-hand side only (written to f_out);
+// STAGE 1..3: the RK3 substeps of STEP (3dmhdsub.f:874-1169).
+// ---------------------------------------------------------------------------
+template <bool MAG, bool ROT, int STAGE>
+__global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
+{
+    constexpr int NQ = NQ_<MAG>::value;
+    extern __shared__ double sm[];
+    const Control* ctl = a.ctl;
+    if (STAGE != 0 && ctl->stop) return;
+
+    const Scalars& s = a.s;
+    const Metrics& m = a.m;
+    const int npx = s.npx, npy = s.npy, npz = s.npz, pitch = s.pitch;
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const int tile = blockIdx.x;
+    const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
+    const int chunk = blockIdx.y;
+    const int k0 = chunk * a.zlen;
+    const int k1 = (chunk == a.nchunks - 1) ? npz : k0 + a.zlen;
+    const int gi = x0 + tx, gj = y0 + ty;
+    const bool active = gi < npx && gj < npy;
+    const int lx = tx + 1, ly = ty + 1;
+
+    // ghost RO copy read by this FLUXES call and the one it leaves behind
+    const int rd = (STAGE == 0) ? ctl->gparity : ((ctl->gparity + STAGE - 1) & 1);
+    const int wr = rd ^ 1;
+
+    const double DT = ctl->dt;
+    const double cu = STAGE == 1 ? s.gam1 * DT : STAGE == 2 ? s.gam2 * DT : s.gam3 * DT;   // COEF for U
+    const double cz = STAGE == 1 ? s.zeta1 * DT : s.zeta2 * DT;                            // COEF for Z
+
+    // tile column metrics
+    const double dxi = active ? m.dxxdx[gi + 1] : 0.0, d2xi = active ? m.d2xxdx2[gi + 1] : 0.0;
+    const double dyj = active ? m.dyydy[gj + 1] : 0.0, d2yj = active ? m.d2yydy2[gj + 1] : 0.0;
+    const double HX = s.hx, H2X = s.h2x, HY = s.hy, H2Y = s.h2y, HZ = s.hz, H2Z = s.h2z;
+    const double C13 = s.c13, C23 = s.c23, C43 = s.c43, OCV = s.ocv, ORE = s.ore;
+
+    // history of new values for BCON (RU, RV, RO, TT) at k-1 and k-2
+    double h1_ru = 0, h1_rv = 0, h1_ro = 0, h1_tt = 0, h2_ru = 0, h2_rv = 0, h2_ro = 0, h2_tt = 0;
+    // new values of the top wall kept until planes 1 and 2 are done
+    double w0_ro = 0, w0_bx = 0, w0_by = 0, w0_bz = 0, w0_tt = 0;
+    // CFL accumulation (stage 3)
+    unsigned long long kw1 = ~0ull, kw2 = ~0ull, kw3 = ~0ull, kw4 = ~0ull, kmu = 0ull;
+    unsigned int bad = 0;
+
+    const size_t gp = (size_t)npy * pitch;
+    const size_t col = (size_t)gj * pitch + gi;
+
+    load_plane<MAG>(a, sm, (k0 - 1 + 3) % 3, k0 - 1, x0, y0, rd);
+    load_plane<MAG>(a, sm, k0 % 3, k0, x0, y0, rd);
+
+    for (int k = k0; k < k1; ++k) {
+        load_plane<MAG>(a, sm, (k + 1) % 3, k + 1, x0, y0, rd);
+        __syncthreads();
+        if (active) {
+            const double* Sm = sm + (size_t)((k + 2) % 3) * NQ * SX * SY;  // plane k-1
+            const double* Sc = sm + (size_t)(k % 3) * NQ * SX * SY;        // plane k
+            const double* Sp = sm + (size_t)((k + 1) % 3) * NQ * SX * SY;  // plane k+1
+#define C_(q, dx, dy) Sc[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
+#define M_(q, dx, dy) Sm[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
+#define P_(q, dx, dy) Sp[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
+            const bool top = (k == 0), bot = (k == npz - 1);
+            const double dzk = m.dzzdz[k + 1], d2zk = m.d2zzdz2[k + 1];
+            const double rka = m.rkapa[k + 1], dka = m.dkapa[k + 1];
+            const double tmpy = HY * dyj, tmpz = HZ * dzk;
+            const double tmpz1 = HZ * d2zk, tmpz2 = H2Z * dzk * dzk;
+            const double tmpy1 = HY * d2yj, tmpy2 = H2Y * dyj * dyj;
+
+            // own-column values two and three planes inside a wall (one-sided stencils)
+            double rw2 = 0, ww2 = 0, bx2 = 0, bx3 = 0, by2 = 0, by3 = 0;
+            if (top || bot) {
+                const int kk2 = top ? 2 : npz - 3, kk3 = top ? 3 : npz - 4;
+                const size_t c2 = (size_t)kk2 * a.pstride + col, c3 = (size_t)kk3 * a.pstride + col;
+                rw2 = a.u_in[c2 + F_RW * a.fstride];
+                const double ro2 = a.u_in[c2 + F_RO * a.fstride];
+                ww2 = rw2 * (1.0 / ro2);
+                if (MAG) {
+                    bx2 = a.u_in[c2 + F_BX * a.fstride];
+                    bx3 = a.u_in[c3 + F_BX * a.fstride];
+                    by2 = a.u_in[c2 + F_BY * a.fstride];
+                    by3 = a.u_in[c3 + F_BY * a.fstride];
+                }
+            }
+
+            const double RUc = C_(Q_RU, 0, 0), RVc = C_(Q_RV, 0, 0), RWc = C_(Q_RW, 0, 0);
+            const double ROc = C_(Q_RO, 0, 0), TTc = C_(Q_TT, 0, 0), RIc = C_(Q_RI, 0, 0);
+            const double UUc = C_(Q_UU, 0, 0), VVc = C_(Q_VV, 0, 0), WWc = C_(Q_WW, 0, 0);
+            const double BXc0 = MAG ? C_(Q_BX, 0, 0) : 0.0, BYc0 = MAG ? C_(Q_BY, 0, 0) : 0.0;
+            const double BZc0 = MAG ? C_(Q_BZ, 0, 0) : 0.0;
+
+            // ---- continuity: loops 10, 40-60, 70 (3dmhdsub.f:1258-1295)
+            double fr = (C_(Q_RU, -1, 0) - C_(Q_RU, 1, 0)) * HX * dxi;
+            fr = fr - (C_(Q_RV, 0, 1) - C_(Q_RV, 0, -1)) * tmpy;
+            double dwz;
+            if (top) dwz = (4.0 * P_(Q_RW, 0, 0) - rw2) * tmpz;
+            else if (bot) dwz = (rw2 - 4.0 * M_(Q_RW, 0, 0)) * tmpz;
+            else dwz = (P_(Q_RW, 0, 0) - M_(Q_RW, 0, 0)) * tmpz;
+            fr = fr - dwz;
+            // ---- buoyancy and pressure gradient: loops 80, 120 (1376-1404)
+            double fw = s.grav * ROc;
+            fw = fw - (P_(Q_P, 0, 0) - M_(Q_P, 0, 0)) * tmpz;
+            double fv = (C_(Q_P, 0, -1) - C_(Q_P, 0, 1)) * tmpy;
+            double fu = (C_(Q_P, -1, 0) - C_(Q_P, 1, 0)) * HX * dxi;
+            // ---- momentum advection: loops 210, 280, 330 (1435-1482)
+            fu = fu - (C_(Q_RU, 1, 0) * C_(Q_UU, 1, 0) - C_(Q_RU, -1, 0) * C_(Q_UU, -1, 0)) * HX * dxi;
+            fu = fu - (C_(Q_RU, 0, 1) * C_(Q_VV, 0, 1) - C_(Q_RU, 0, -1) * C_(Q_VV, 0, -1)) * tmpy;
+            fu = fu - (P_(Q_RU, 0, 0) * P_(Q_WW, 0, 0) - M_(Q_RU, 0, 0) * M_(Q_WW, 0, 0)) * tmpz;
+            fv = fv - (C_(Q_RV, 1, 0) * C_(Q_UU, 1, 0) - C_(Q_RV, -1, 0) * C_(Q_UU, -1, 0)) * HX * dxi;
+            fv = fv - (C_(Q_RV, 0, 1) * C_(Q_VV, 0, 1) - C_(Q_RV, 0, -1) * C_(Q_VV, 0, -1)) * tmpy;
+            fv = fv - (P_(Q_RV, 0, 0) * P_(Q_WW, 0, 0) - M_(Q_RV, 0, 0) * M_(Q_WW, 0, 0)) * tmpz;
+            fw = fw - (C_(Q_RW, 1, 0) * C_(Q_UU, 1, 0) - C_(Q_RW, -1, 0) * C_(Q_UU, -1, 0)) * HX * dxi;
+            fw = fw - (C_(Q_RW, 0, 1) * C_(Q_VV, 0, 1) - C_(Q_RW, 0, -1) * C_(Q_VV, 0, -1)) * tmpy;
+            fw = fw - (P_(Q_RW, 0, 0) * P_(Q_WW, 0, 0) - M_(Q_RW, 0, 0) * M_(Q_WW, 0, 0)) * tmpz;
+            // ---- temperature advection: loop 450 (1495-1506)
+            double ft = -(1.0 * UUc * (C_(Q_TT, 1, 0) - C_(Q_TT, -1, 0)) * HX * dxi);
+            ft = ft - VVc * (C_(Q_TT, 0, 1) - C_(Q_TT, 0, -1)) * tmpy;
+            ft = ft - WWc * (P_(Q_TT, 0, 0) - M_(Q_TT, 0, 0)) * tmpz;
+            // ---- conduction, non-LREM: loop 519 (1583-1611)
+            {
+                const double TMP = s.tmp_cond;
+                const double txp = C_(Q_TT, 1, 0), txm = C_(Q_TT, -1, 0);
+                const double typ = C_(Q_TT, 0, 1), tym = C_(Q_TT, 0, -1);
+                const double tzp = P_(Q_TT, 0, 0), tzm = M_(Q_TT, 0, 0);
+                ft = ft + ((txp - txm) * HX * d2xi + (txp - 2.0 * TTc + txm) * H2X * dxi * dxi) * RIc * TMP * rka;
+                ft = ft + ((typ - tym) * tmpy1 + (typ - 2.0 * TTc + tym) * tmpy2) * RIc * TMP * rka;
+                ft = ft + ((tzp - tzm) * tmpz1 + (tzp - 2.0 * TTc + tzm) * tmpz2) * RIc * TMP * rka;
+                ft = ft + (tzp - tzm) * HZ * dzk * RIc * TMP * dka;
+            }
+            // ---- viscous momentum terms: loops 530, 540, 550 (1818-1886)
+            {
+                const double uxp = C_(Q_UU, 1, 0), uxm = C_(Q_UU, -1, 0), uyp = C_(Q_UU, 0, 1), uym = C_(Q_UU, 0, -1);
+                const double uzp = P_(Q_UU, 0, 0), uzm = M_(Q_UU, 0, 0);
+                fu = fu + ORE * (C43 * ((uxp - uxm) * HX * d2xi + (uxp - 2.0 * UUc + uxm) * H2X * dxi * dxi)
+                                 + (uyp - uym) * tmpy1 + (uyp - 2.0 * UUc + uym) * tmpy2
+                                 + (uzp - uzm) * tmpz1 + (uzp - 2.0 * UUc + uzm) * tmpz2);
+                const double vxp = C_(Q_VV, 1, 0), vxm = C_(Q_VV, -1, 0), vyp = C_(Q_VV, 0, 1), vym = C_(Q_VV, 0, -1);
+                const double vzp = P_(Q_VV, 0, 0), vzm = M_(Q_VV, 0, 0);
+                fv = fv + ORE * ((vxp - vxm) * HX * d2xi + (vxp - 2.0 * VVc + vxm) * H2X * dxi * dxi
+                                 + C43 * ((vyp - vym) * tmpy1 + (vyp - 2.0 * VVc + vym) * tmpy2)
+                                 + (vzp - vzm) * tmpz1 + (vzp - 2.0 * VVc + vzm) * tmpz2);
+                const double wxp = C_(Q_WW, 1, 0), wxm = C_(Q_WW, -1, 0), wyp = C_(Q_WW, 0, 1), wym = C_(Q_WW, 0, -1);
+                const double wzp = P_(Q_WW, 0, 0), wzm = M_(Q_WW, 0, 0);
+                fw = fw + ORE * ((wxp - wxm) * HX * d2xi + (wxp - 2.0 * WWc + wxm) * H2X * dxi * dxi
+                                 + (wyp - wym) * tmpy1 + (wyp - 2.0 * WWc + wym) * tmpy2
+                                 + C43 * ((wzp - wzm) * tmpz1 + (wzp - 2.0 * WWc + wzm) * tmpz2));
+            }
+            // ---- viscous and compressional heating, (1/3)grad(div u): loops 650-940 (1891-2101)
+            const double TA = s.tmp_a, TB = s.tmp_b, T13 = s.tmp_13;
+            const double ux = (C_(Q_UU, 1, 0) - C_(Q_UU, -1, 0)) * HX * dxi;
+            const double ux_p = (C_(Q_UU, 1, 1) - C_(Q_UU, -1, 1)) * HX * dxi;
+            const double ux_m = (C_(Q_UU, 1, -1) - C_(Q_UU, -1, -1)) * HX * dxi;
+            const double vx = (C_(Q_VV, 1, 0) - C_(Q_VV, -1, 0)) * HX * dxi;
+            const double vx_p = (C_(Q_VV, 1, 1) - C_(Q_VV, -1, 1)) * HX * dxi;
+            const double vx_m = (C_(Q_VV, 1, -1) - C_(Q_VV, -1, -1)) * HX * dxi;
+            const double wx = (C_(Q_WW, 1, 0) - C_(Q_WW, -1, 0)) * HX * dxi;
+            ft = ft + (C43 * ux * ux + vx * vx + wx * wx) * RIc * TA;             // 700
+            ft = ft - OCV * ux * TTc;                                            // 710
+            fu = fu + T13 * (vx_p - vx_m) * HY * dyj;                            // 720
+            fv = fv + T13 * (ux_p - ux_m) * HY * dyj;                            // 730
+            const double uy = (C_(Q_UU, 0, 1) - C_(Q_UU, 0, -1)) * HY * dyj;     // 740
+            ft = ft + (uy * uy + 2.0 * uy * vx) * RIc * TA;                      // 750
+            const double vy = (C_(Q_VV, 0, 1) - C_(Q_VV, 0, -1)) * HY * dyj;     // 755
+            ft = ft + vy * vy * RIc * TB;                                        // 760
+            ft = ft - OCV * vy * TTc;                                            // 770
+            const double wz = (P_(Q_WW, 0, 0) - M_(Q_WW, 0, 0)) * HZ * dzk;      // 790
+            const double wz_xp = (P_(Q_WW, 1, 0) - M_(Q_WW, 1, 0)) * HZ * dzk;
+            const double wz_xm = (P_(Q_WW, -1, 0) - M_(Q_WW, -1, 0)) * HZ * dzk;
+            const double wz_yp = (P_(Q_WW, 0, 1) - M_(Q_WW, 0, 1)) * HZ * dzk;
+            const double wz_ym = (P_(Q_WW, 0, -1) - M_(Q_WW, 0, -1)) * HZ * dzk;
+            ft = ft + (wz * wz - ux * wz - ux * vy - vy * wz) * RIc * TB;        // 820
+            ft = ft - OCV * wz * TTc;                                            // 830
+            fu = fu + T13 * (wz_xp - wz_xm) * HX * dxi;                          // 840
+            fv = fv + T13 * (wz_yp - wz_ym) * HY * dyj;                          // 850
+            const double uz = (P_(Q_UU, 0, 0) - M_(Q_UU, 0, 0)) * HZ * dzk;      // 860
+            const double uz_xp = (P_(Q_UU, 1, 0) - M_(Q_UU, 1, 0)) * HZ * dzk;
+            const double uz_xm = (P_(Q_UU, -1, 0) - M_(Q_UU, -1, 0)) * HZ * dzk;
+            const double vz = (P_(Q_VV, 0, 0) - M_(Q_VV, 0, 0)) * HZ * dzk;      // 880
+            const double vz_yp = (P_(Q_VV, 0, 1) - M_(Q_VV, 0, 1)) * HZ * dzk;
+            const double vz_ym = (P_(Q_VV, 0, -1) - M_(Q_VV, 0, -1)) * HZ * dzk;
+            const double wy = (C_(Q_WW, 0, 1) - C_(Q_WW, 0, -1)) * HY * dyj;     // 900
+            ft = ft + (uz * uz + vz * vz + wy * wy + 2.0 * vz * wy) * RIc * TA;  // 910
+            fw = fw + T13 * ((uz_xp - uz_xm) * HX * dxi + (vz_yp - vz_ym) * HY * dyj);  // 920
+            ft = ft + 2.0 * uz * wx * RIc * TA;                                  // 940
+            // ---- Coriolis: loops 950-970 (2106-2125)
+            if (ROT) {
+                fu = fu + s.omz * RVc;
+                fv = fv - s.omz * RUc + s.omx * RWc;
+                fw = fw - s.omx * RVc;
+            }
+            // ---- induction, Lorentz force, Ohmic heating: 2129-2634
+            double w1 = 0, w2 = 0, w3 = 0;
+            if (MAG) {
+                const double OBETA = s.obeta, ORM = s.orm, TM = s.tmp_m;
+                const double BXc = C_(Q_BX, 0, 0), BYc = C_(Q_BY, 0, 0), BZc = C_(Q_BZ, 0, 0);
+                w2 = BXc * vx - BYc * ux;                                        // 1030
+                w3 = BXc * wx - BZc * ux;                                        // 1040
+                w1 = BYc * uy - BXc * vy;                                        // 1080
+                w3 = w3 + BYc * wy - BZc * vy;                                   // 1090
+                double wzm = wz;                                                 // 1120
+                if (top) wzm = (4.0 * P_(Q_WW, 0, 0) - ww2) * HZ * dzk;          // 1125
+                else if (bot) wzm = (ww2 - 4.0 * M_(Q_WW, 0, 0)) * HZ * dzk;     // 1126
+                w1 = w1 + BZc * uz - BXc * wzm;                                  // 1130
+                w2 = w2 + BZc * vz - BYc * wzm;                                  // 1140
+                const double bxxp = C_(Q_BX, 1, 0), bxxm = C_(Q_BX, -1, 0);
+                const double byxp = C_(Q_BY, 1, 0), byxm = C_(Q_BY, -1, 0);
+                const double bzxp = C_(Q_BZ, 1, 0), bzxm = C_(Q_BZ, -1, 0);
+                const double bxyp = C_(Q_BX, 0, 1), bxym = C_(Q_BX, 0, -1);
+                const double byyp = C_(Q_BY, 0, 1), byym = C_(Q_BY, 0, -1);
+                const double bzyp = C_(Q_BZ, 0, 1), bzym = C_(Q_BZ, 0, -1);
+                const double bxzp = P_(Q_BX, 0, 0), bxzm = M_(Q_BX, 0, 0);
+                const double byzp = P_(Q_BY, 0, 0), byzm = M_(Q_BY, 0, 0);
+                const double bzzp = P_(Q_BZ, 0, 0), bzzm = M_(Q_BZ, 0, 0);
+                const double bxx = (bxxp - bxxm) * HX * dxi;                     // 1150
+                const double byx = (byxp - byxm) * HX * dxi;                     // 1160
+                const double bzx = (bzxp - bzxm) * HX * dxi;                     // 1170
+                const double bxy = (bxyp - bxym) * HY * dyj;                     // 1180
+                fu = fu + OBETA * BYc * (bxy - byx) - OBETA * BZc * bzx;         // 1190
+                fv = fv + OBETA * BXc * (byx - bxy);                             // 1200
+                fw = fw + OBETA * BXc * bzx;                                     // 1210
+                ft = ft + (bxy * bxy + byx * byx + bzx * bzx - 2.0 * byx * bxy) * RIc * TM;  // 1220
+                w1 = w1 - UUc * bxx - VVc * bxy;                                 // 1230
+                w2 = w2 - UUc * byx;                                             // 1240
+                w3 = w3 - UUc * bzx;                                             // 1250
+                const double bxx2 = (bxxp - bxxm) * HX * d2xi + (bxxp - 2.0 * BXc + bxxm) * H2X * dxi * dxi;  // 1260
+                const double byx2 = (byxp - byxm) * HX * d2xi + (byxp - 2.0 * BYc + byxm) * H2X * dxi * dxi;  // 1265
+                const double bxy2 = (bxyp - bxym) * HY * d2yj + (bxyp - 2.0 * BXc + bxym) * H2Y * dyj * dyj;  // 1270
+                w1 = w1 + ORM * (bxx2 + bxy2);                                   // 1280
+                w2 = w2 + ORM * byx2;                                            // 1290
+                const double bzx2 = (bzxp - bzxm) * HX * d2xi + (bzxp - 2.0 * BZc + bzxm) * H2X * dxi * dxi;  // 1300
+                w3 = w3 + ORM * bzx2;                                            // 1310
+                const double bxz = (bxzp - bxzm) * HZ * dzk;                     // 1320
+                const double byy = (byyp - byym) * HY * dyj;                     // 1330
+                fu = fu + OBETA * BZc * bxz;                                     // 1340
+                fw = fw - OBETA * BXc * bxz;                                     // 1350
+                ft = ft + (bxz * bxz - 2.0 * bxz * bzx) * RIc * TM;              // 1360
+                w1 = w1 - WWc * bxz;                                             // 1370
+                w2 = w2 - VVc * byy;                                             // 1380
+                double bxz2;                                                     // 1390-1392
+                if (top)
+                    bxz2 = (-3.0 * BXc + 4.0 * bxzp - bx2) * HZ * d2zk
+                         + (2.0 * BXc - 5.0 * bxzp + 4.0 * bx2 - bx3) * H2Z * dzk * dzk;
+                else if (bot)
+                    bxz2 = (3.0 * BXc - 4.0 * bxzm + bx2) * HZ * d2zk
+                         + (2.0 * BXc - 5.0 * bxzm + 4.0 * bx2 - bx3) * H2Z * dzk * dzk;
+                else
+                    bxz2 = (bxzp - bxzm) * HZ * d2zk + (bxzp - 2.0 * BXc + bxzm) * H2Z * dzk * dzk;
+                const double byy2 = (byyp - byym) * HY * d2yj + (byyp - 2.0 * BYc + byym) * H2Y * dyj * dyj;  // 1400
+                w1 = w1 + ORM * bxz2;                                            // 1410
+                w2 = w2 + ORM * byy2;                                            // 1420
+                const double byz = (byzp - byzm) * HZ * dzk;                     // 1430
+                const double bzy = (bzyp - bzym) * HY * dyj;                     // 1440
+                const double cur = byz - bzy;                                    // 1450
+                fv = fv + OBETA * BZc * cur;                                     // 1460
+                fw = fw - OBETA * BYc * cur;                                     // 1470
+                ft = ft + (byz * byz + bzy * bzy - 2.0 * byz * bzy) * RIc * TM;  // 1480
+                w2 = w2 - WWc * byz;                                             // 1490
+                w3 = w3 - VVc * bzy;                                             // 1500
+                double byz2;                                                     // 1510-1513
+                if (top)
+                    byz2 = (-3.0 * BYc + 4.0 * byzp - by2) * HZ * d2zk
+                         + (2.0 * BYc - 5.0 * byzp + 4.0 * by2 - by3) * H2Z * dzk * dzk;
+                else if (bot)
+                    byz2 = (3.0 * BYc - 4.0 * byzm + by2) * HZ * d2zk
+                         + (2.0 * BYc - 5.0 * byzm + 4.0 * by2 - by3) * H2Z * dzk * dzk;
+                else
+                    byz2 = (byzp - byzm) * HZ * d2zk + (byzp - 2.0 * BYc + byzm) * H2Z * dzk * dzk;
+                const double bzy2 = (bzyp - bzym) * HY * d2yj + (bzyp - 2.0 * BZc + bzym) * H2Y * dyj * dyj;  // 1520
+                w2 = w2 + ORM * byz2;                                            // 1530
+                w3 = w3 + ORM * bzy2;                                            // 1540
+                const double bzz = (bzzp - bzzm) * HZ * dzk;                     // 1550
+                w3 = w3 - WWc * bzz;                                             // 1560
+                const double bzz2 = (bzzp - bzzm) * HZ * d2zk + (bzzp - 2.0 * BZc + bzzm) * H2Z * dzk * dzk;  // 1570
+                w3 = w3 + ORM * bzz2;                                            // 1580
+            }
+            // ghost RO planes: this FLUXES call leaves 1/RO behind (3dmhdsub.f:1386-1391)
+            if (STAGE != 0) {
+                if (top) a.gro[(size_t)wr * 2 * gp + col] = M_(Q_RI, 0, 0);
+                if (bot) a.gro[(size_t)wr * 2 * gp + gp + col] = P_(Q_RI, 0, 0);
+            }
+#undef C_
+#undef M_
+#undef P_
+            const size_t c = (size_t)k * a.pstride + col;
+            const bool wall = top || bot;
+            if (STAGE == 0) {
+                // right-hand sides; values BCON discards on the walls are reported as 0
+                a.f_out[c + 0 * a.fstride] = wall ? 0.0 : fu;
+                a.f_out[c + 1 * a.fstride] = wall ? 0.0 : fv;
+                a.f_out[c + 2 * a.fstride] = wall ? 0.0 : fw;
+                a.f_out[c + 3 * a.fstride] = fr;
+                a.f_out[c + 4 * a.fstride] = wall ? 0.0 : ft;
+                if (MAG) {
+                    a.f_out[c + 5 * a.fstride] = w1;
+                    a.f_out[c + 6 * a.fstride] = w2;
+                    a.f_out[c + 7 * a.fstride] = wall ? 0.0 : w3;
+                }
+            } else {
+                // ---- RK3 update: U = Z + COEF*F (STEP loops 70-140, 270-340, 470-540);
+                //      stage 1 has Z = U (loops 71-141)
+                double zu, zv, zw, zr, zt, zbx = 0, zby = 0, zbz = 0;
+                if (STAGE == 1) {
+                    zu = RUc; zv = RVc; zw = RWc; zr = ROc; zt = TTc;
+                    if (MAG) { zbx = BXc0; zby = BYc0; zbz = BZc0; }
+                } else {
+                    zu = a.z[c + F_RU * a.fstride];
+                    zv = a.z[c + F_RV * a.fstride];
+                    zw = a.z[c + F_RW * a.fstride];
+                    zt = a.z[c + F_TT * a.fstride];
+                    zr = a.z[c + F_RO * a.fstride];
+                    if (MAG) {
+                        zbx = a.z[c + F_BX * a.fstride];
+                        zby = a.z[c + F_BY * a.fstride];
+                        zbz = a.z[c + F_BZ * a.fstride];
+                    }
+                }
+                const double nu = zu + cu * fu, nv = zv + cu * fv, nw = zw + cu * fw;
+                const double nr = zr + cu * fr, nt = zt + cu * ft;
+                const double nbx = zbx + cu * w1, nby = zby + cu * w2, nbz = zbz + cu * w3;
+                double* uo = a.u_out + c;
+                uo[F_RO * a.fstride] = nr;
+                if (MAG) {
+                    uo[F_BX * a.fstride] = nbx;
+                    uo[F_BY * a.fstride] = nby;
+                }
+                if (!wall) {
+                    uo[F_RU * a.fstride] = nu;
+                    uo[F_RV * a.fstride] = nv;
+                    uo[F_RW * a.fstride] = nw;
+                    uo[F_TT * a.fstride] = nt;
+                    if (MAG) uo[F_BZ * a.fstride] = nbz;
+                }
+                // ---- Z for the next stage: Z = U + ZETA*DT*F (loops 190-260, 390-460).
+                //      On the walls only RO, BX, BY are ever read back.
+                if (STAGE < 3) {
+                    double* zo = a.z + c;
+                    zo[F_RO * a.fstride] = nr + cz * fr;
+                    if (MAG) {
+                        zo[F_BX * a.fstride] = nbx + cz * w1;
+                        zo[F_BY * a.fstride] = nby + cz * w2;
+                    }
+                    if (!wall) {
+                        zo[F_RU * a.fstride] = nu + cz * fu;
+                        zo[F_RV * a.fstride] = nv + cz * fv;
+                        zo[F_RW * a.fstride] = nw + cz * fw;
+                        zo[F_TT * a.fstride] = nt + cz * ft;
+                        if (MAG) zo[F_BZ * a.fstride] = nbz + cz * w3;
+                    }
+                }
+                // ---- BCON (3dmhdsub.f:2751-2955) and the CFL parts of the next step
+                if (top) {
+                    w0_ro = nr; w0_bx = nbx; w0_by = nby; w0_bz = nbz; w0_tt = nt;
+                } else if (!bot) {
+                    if (STAGE == 3) {
+                        CflPart cp;
+                        cfl_cell<MAG>(s, nu, nv, nw, nr, nt, nbx, nby, nbz, cell_dd(m, gi, gj, k), rka, cp);
+                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
+                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
+                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
+                    }
+                }
+                if (k == 2 && k0 == 0) {
+                    // top wall: new values of planes K=3 (h1) and K=4 (this plane)
+                    const double ru_w = w0_ro * (C43 * h1_ru / h1_ro - C13 * nu / nr);
+                    const double rv_w = w0_ro * (C43 * h1_rv / h1_ro - C13 * nv / nr);
+                    double tt_w = w0_tt;
+                    if (s.plume) {
+                        const double tpr = (s.tc != 0.0) ? s.tp + (1.0 - s.tp) * exp(-ctl->timt / s.tc) : s.tp;
+                        const double gx = m.plume_gx[gi + 1], gy = m.plume_gy[gj + 1];
+                        if (s.itcon == 0) tt_w = 1.0 - (1.0 - tpr) * gx / s.hh * gy / s.hh;
+                        else tt_w = C43 * h1_tt - C13 * nt - C23 * s.top_dz * (s.theta - (s.theta - tpr) * gx / s.hh * gy / s.hh);
+                    } else if (s.itcon == 0 || s.itcon == 2 || s.itcon == 4) {
+                        tt_w = 1.0;
+                        if (s.itcon == 4 && gi + 2 <= (npx + 2) / 2) tt_w = 1.0 - s.tp;
+                    } else if (s.itcon == 1) {
+                        tt_w = C43 * h1_tt - C13 * nt - s.top_flux;
+                    }
+                    const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : w0_bz;
+                    const size_t c0 = col;
+                    double* u0 = a.u_out + c0;
+                    u0[F_RU * a.fstride] = ru_w;
+                    u0[F_RV * a.fstride] = rv_w;
+                    u0[F_RW * a.fstride] = 0.0;
+                    u0[F_TT * a.fstride] = tt_w;
+                    if (MAG) u0[F_BZ * a.fstride] = bz_w;
+                    if (STAGE == 3) {
+                        CflPart cp;
+                        cfl_cell<MAG>(s, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w, cell_dd(m, gi, gj, 0),
+                                      m.rkapa[1], cp);
+                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
+                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
+                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
+                    }
+                }
+                if (bot) {
+                    // bottom wall: new values of planes K=NZ-2 (h1) and K=NZ-3 (h2)
+                    const double ru_w = nr * (C43 * h1_ru / h1_ro - C13 * h2_ru / h2_ro);
+                    const double rv_w = nr * (C43 * h1_rv / h1_ro - C13 * h2_rv / h2_ro);
+                    const double tt_w = (s.izcon == 0) ? s.tb : C43 * h1_tt - C13 * h2_tt + s.bot_flux;
+                    const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : nbz;
+                    uo[F_RU * a.fstride] = ru_w;
+                    uo[F_RV * a.fstride] = rv_w;
+                    uo[F_RW * a.fstride] = 0.0;
+                    uo[F_TT * a.fstride] = tt_w;
+                    if (MAG) uo[F_BZ * a.fstride] = bz_w;
+                    if (STAGE == 3) {
+                        CflPart cp;
+                        cfl_cell<MAG>(s, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w, cell_dd(m, gi, gj, k), rka, cp);
+                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
+                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
+                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
+                    }
+                }
+                h2_ru = h1_ru; h2_rv = h1_rv; h2_ro = h1_ro; h2_tt = h1_tt;
+                h1_ru = nu; h1_rv = nv; h1_ro = nr; h1_tt = nt;
+            }
+        }
+        __syncthreads();
+    }
+    if (STAGE == 3) {
+        __shared__ unsigned long long red[(NT / 32) * 6];
+        cfl_commit(a.acc, kw1, kw2, kw3, kw4, kmu, bad, red);
+    }
+}
+
+// Standalone CFL reduction over the current state (STEP 3dmhdsub.f:741-873),
+// used before the first step and after a state change.
+template <bool MAG>
+__global__ void __launch_bounds__(NT) k_cfl(const StageArgs a)
+{
+    const Scalars& s = a.s;
+    const int npx = s.npx, npy = s.npy, npz = s.npz;
+    const size_t ncell = (size_t)npx * npy * npz;
+    unsigned long long kw1 = ~0ull, kw2 = ~0ull, kw3 = ~0ull, kw4 = ~0ull, kmu = 0ull;
+    unsigned int bad = 0;
+    for (size_t q = (size_t)blockIdx.x * NT + threadIdx.x; q < ncell; q += (size_t)gridDim.x * NT) {
+        const int gi = (int)(q % npx);
+        const int gj = (int)((q / npx) % npy);
+        const int k = (int)(q / ((size_t)npx * npy));
+        const size_t c = (size_t)k * a.pstride + (size_t)gj * s.pitch + gi;
+        const double* u = a.u_in + c;
+        CflPart cp;
+        cfl_cell<MAG>(s, u[F_RU * a.fstride], u[F_RV * a.fstride], u[F_RW * a.fstride], u[F_RO * a.fstride],
+                      u[F_TT * a.fstride], MAG ? u[F_BX * a.fstride] : 0.0, MAG ? u[F_BY * a.fstride] : 0.0,
+                      MAG ? u[F_BZ * a.fstride] : 0.0, cell_dd(a.m, gi, gj, k), a.m.rkapa[k + 1], cp);
+        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
+        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
+        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
+    }
+    __shared__ unsigned long long red[(NT / 32) * 6];
+    cfl_commit(a.acc, kw1, kw2, kw3, kw4, kmu, bad, red);
+}
+
+// Standalone BCON on the current state, in place (test entry point).
+template <bool MAG>
+__global__ void __launch_bounds__(NT) k_bcon(const StageArgs a)
+{
+    const Scalars& s = a.s;
+    const int npx = s.npx, npy = s.npy, npz = s.npz;
+    const int q = blockIdx.x * NT + threadIdx.x;
+    if (q >= npx * npy) return;
+    const int gi = q % npx, gj = q / npx;
+    const size_t col = (size_t)gj * s.pitch + gi;
+    double* u = const_cast<double*>(a.u_in);
+    auto at = [&](int f, int k) -> double& { return u[(size_t)f * a.fstride + (size_t)k * a.pstride + col]; };
+    const double C13 = s.c13, C23 = s.c23, C43 = s.c43;
+    // top
+    {
+        const double ro0 = at(F_RO, 0), ro1 = at(F_RO, 1), ro2 = at(F_RO, 2);
+        const double ru_w = ro0 * (C43 * at(F_RU, 1) / ro1 - C13 * at(F_RU, 2) / ro2);
+        const double rv_w = ro0 * (C43 * at(F_RV, 1) / ro1 - C13 * at(F_RV, 2) / ro2);
+        double tt_w = at(F_TT, 0);
+        const double t1 = at(F_TT, 1), t2 = at(F_TT, 2);
+        if (s.plume) {
+            const double tpr = (s.tc != 0.0) ? s.tp + (1.0 - s.tp) * exp(-a.ctl->timt / s.tc) : s.tp;
+            const double gx = a.m.plume_gx[gi + 1], gy = a.m.plume_gy[gj + 1];
+            if (s.itcon == 0) tt_w = 1.0 - (1.0 - tpr) * gx / s.hh * gy / s.hh;
+            else tt_w = C43 * t1 - C13 * t2 - C23 * s.top_dz * (s.theta - (s.theta - tpr) * gx / s.hh * gy / s.hh);
+        } else if (s.itcon == 0 || s.itcon == 2 || s.itcon == 4) {
+            tt_w = 1.0;
+            if (s.itcon == 4 && gi + 2 <= (npx + 2) / 2) tt_w = 1.0 - s.tp;
+        } else if (s.itcon == 1) {
+            tt_w = C43 * t1 - C13 * t2 - s.top_flux;
+        }
+        at(F_RU, 0) = ru_w;
+        at(F_RV, 0) = rv_w;
+        at(F_RW, 0) = 0.0;
+        at(F_TT, 0) = tt_w;
+        if (MAG && s.ibcon == 0) at(F_BZ, 0) = 0.0;
+    }
+    // bottom
+    {
+        const int kb = npz - 1;
+        const double ro0 = at(F_RO, kb), ro1 = at(F_RO, kb - 1), ro2 = at(F_RO, kb - 2);
+        const double ru_w = ro0 * (C43 * at(F_RU, kb - 1) / ro1 - C13 * at(F_RU, kb - 2) / ro2);
+        const double rv_w = ro0 * (C43 * at(F_RV, kb - 1) / ro1 - C13 * at(F_RV, kb - 2) / ro2);
+        const double tt_w = (s.izcon == 0) ? s.tb : C43 * at(F_TT, kb - 1) - C13 * at(F_TT, kb - 2) + s.bot_flux;
+        at(F_RU, kb) = ru_w;
+        at(F_RV, kb) = rv_w;
+        at(F_RW, kb) = 0.0;
+        at(F_TT, kb) = tt_w;
+        if (MAG && s.ibcon == 0) at(F_BZ, kb) = 0.0;
+    }
+}
+
+template <bool MAG, bool ROT>
+static cudaError_t launch_stage_t(int stage, const StageArgs& a, cudaStream_t st)
+{
+    constexpr int NQ = NQ_<MAG>::value;
+    const size_t smem = (size_t)3 * NQ * SX * SY * sizeof(double);
+    const int nty = (a.s.npy + TY - 1) / TY;
+    dim3 grid(a.ntx * nty, a.nchunks);
+    switch (stage) {
+#define L_(S)                                                                                          \
+    case S: {                                                                                          \
+        cudaFuncSetAttribute(k_stage<MAG, ROT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        k_stage<MAG, ROT, S><<<grid, NT, smem, st>>>(a);                                              \
+        break;                                                                                         \
+    }
+        L_(0) L_(1) L_(2) L_(3)
+#undef L_
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int stage, const StageArgs& a, cudaStream_t st)
+{
+    if (a.s.lmag) return a.s.lrot ? launch_stage_t<true, true>(stage, a, st) : launch_stage_t<true, false>(stage, a, st);
+    return a.s.lrot ? launch_stage_t<false, true>(stage, a, st) : launch_stage_t<false, false>(stage, a, st);
+}
+
+cudaError_t launch_cfl(const StageArgs& a, cudaStream_t st)
+{
+    const size_t ncell = (size_t)a.s.npx * a.s.npy * a.s.npz;
+    size_t nb = (ncell + NT - 1) / NT;
+    if (nb > 148 * 8) nb = 148 * 8;
+    if (a.s.lmag) k_cfl<true><<<(unsigned)nb, NT, 0, st>>>(a);
+    else k_cfl<false><<<(unsigned)nb, NT, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bcon(const StageArgs& a, cudaStream_t st)
+{
+    const int n = a.s.npx * a.s.npy;
+    const int nb = (n + NT - 1) / NT;
+    if (a.s.lmag) k_bcon<true><<<nb, NT, 0, st>>>(a);
+    else k_bcon<false><<<nb, NT, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace MHD3D_NS
+}  // namespace mhd3d
