@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the 3dmhd time step on B200: Mcell-RK3-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the FP64-plain fine run of the learned-closure case, 512x512x256,
+rotating MHD polytrope (Ra=1e6, Ta=1e6, Pr=1, Pm=4, density contrast 10,
+beta=1e4, tanh z stretch 1.5), set up by the host mirror of the reference
+driver (STATIC + TUBE model 4 + RAN2 perturbation).  One "step" is one
+full RK3 step (one CALL STEP).
+
+value  : cells x steps / device time, time from CUDA events on the stream
+         the kernels run on, max over ranks; N>1 runs independent replicas
+         (the single-GPU path does not shard across GPUs).
+e2e    : the same metric through the public C-ABI with host buffers:
+         mhd3d_upload from pinned host memory, K x mhd3d_step(1) (each reads
+         DT/TIMC/TIMT/UMACH/NIT back, as the driver's DT check needs), and
+         mhd3d_download to pinned host memory, all inside the timed region.
+roofline: the fused stage kernel, algorithmic bytes 10*nf*8 per cell and
+         step (compulsory U/Z traffic), against the measured HBM copy peak.
+cpu_baseline: the reference's own step (translated build in oracle/_ref)
+         on a bounded 512x512x32 slab of the same physics, all host cores.
+--impl reference: the reference's CPU step timed on the host cores for the
+         same metric (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rast-3dmhd_b200"))
+
+METRIC = "Mcell-RK3-steps/s at 512²×256: FP32+closure vs FP64 plain, same flux error"
+UNIT = "Mcell-RK3-steps/s"
+WORKLOAD = dict(npx=512, npy=512, npz=256, ra=1e6, ta=1e6, pr=1.0, pm=4.0, contrast=10.0, m=1.0, beta=1e4,
+                stretch=1.5, ampt=2e-4)
+WORKLOAD_NAME = ("FP64-plain fine run of the closure case: 512x512x256 rotating MHD polytrope, "
+                 "Ra=1e6 Ta=1e6 Pr=1 Pm=4 contrast 10 beta=1e4 tanh stretch 1.5")
+SAMPLE_NPZ = 32  # CPU baseline slab
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.tmp.read().strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.tmp.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pow2_floor(n):
+    p = 1
+    while p * 2 <= n:
+        p *= 2
+    return p
+
+
+def decomposition(cores, npy, npz):
+    """NPEY x NPEZ for the reference's own MPI layout: powers of two, >=4 z planes per rank."""
+    p = pow2_floor(max(1, cores))
+    npez = 1
+    while npez * 2 <= p and npz // (npez * 2) >= 4 and npz % (npez * 2) == 0:
+        npez *= 2
+    npey = p // npez
+    while npey > 1 and npy % npey:
+        npey //= 2
+    return npey, npez
+
+
+def cpu_reference_run(steps: int, warmup: int, npz: int = SAMPLE_NPZ):
+    """Time the reference's own step (translated build) on a 512x512xnpz slab, all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mhd3d
+    import oracle_py
+    w = dict(WORKLOAD, npz=npz)
+    cfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
+                                  w["m"], w["beta"], w["stretch"], w["ampt"])
+    setup = mhd3d.make_setup(cfg)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    cells = w["npx"] * w["npy"] * w["npz"]
+    if oracle_py.reference_available():
+        npey, npez = decomposition(cores, w["npy"], w["npz"])
+        r = oracle_py.run_reference(setup.params, setup.grid, setup.state, steps, npey=npey, npez=npez,
+                                    warmup=warmup)
+        secs = r["seconds"]
+        kind, used = "reference", npey * npez
+        how = f"translated reference STEP, {npey}x{npez} MPI ranks (emulated)"
+    else:
+        oracle_py.set_threads(cores)
+        o = oracle_py.Oracle(setup.params, setup.grid, setup.state)
+        o.step(warmup)
+        t0 = time.perf_counter()
+        o.step(steps)
+        secs = time.perf_counter() - t0
+        kind, used = "port", oracle_py.oracle_lib().oracle_get_threads()
+        how = "C restatement (oracle), OpenMP"
+    value = cells * steps / secs / 1e6
+    return {"value": value, "unit": UNIT, "cores": used, "kind": kind,
+            "sample": f"{w['npx']}x{w['npy']}x{w['npz']} slab of the same physics, {warmup} warm-up + {steps} timed "
+                      f"RK3 steps, {how}; {secs:.2f} s"}
+
+
+def run_reference_arm(args, rank, world):
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (host set-up of the reference's STATIC/TUBE/RAN2)",
+            "config": {"workload": WORKLOAD_NAME, "grid": [WORKLOAD["npx"], WORKLOAD["npy"], WORKLOAD["npz"]],
+                       "parallelism": "reference MPI decomposition on the host cores"}}
+    if rank != 0:
+        return None
+    try:
+        cb = cpu_reference_run(args.steps, args.warmup, npz=args.ref_npz)
+    except Exception as e:  # noqa: BLE001
+        return {"impl": "reference", "unavailable": f"reference CPU step failed: {e}"[:300]}
+    line["value"] = cb["value"]
+    line["ms_per_step"] = WORKLOAD["npx"] * WORKLOAD["npy"] * WORKLOAD["npz"] / (cb["value"] * 1e6) * 1e3
+    line["cpu_baseline"] = cb
+    line["e2e"] = {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--grid", type=str, default=None, help="override NPXxNPYxNPZ (testing)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-npz", type=int, default=SAMPLE_NPZ)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        line = run_reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    import numpy as np
+    import torch
+    import mhd3d
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    w = dict(WORKLOAD)
+    if args.grid:
+        w["npx"], w["npy"], w["npz"] = (int(v) for v in args.grid.lower().split("x"))
+    cfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
+                                  w["m"], w["beta"], w["stretch"], w["ampt"], seed=62659 + rank)
+    setup = mhd3d.make_setup(cfg)
+    cells = w["npx"] * w["npy"] * w["npz"]
+    nf = 8 if cfg.lmag else 5
+    mode = mhd3d.MODE_FAST if args.mode == "fast" else mhd3d.MODE_EXACT
+    sim = mhd3d.GpuSim(setup, mode=mode)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(setup.state)
+
+    # warm-up (also builds DT of the first timed step)
+    sim.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput -------------------------------------
+    clocks = ClockSampler(local) if rank == 0 else None
+    sim.profile(True)
+    sim.profile_read()
+    barrier()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    res = sim.sync()
+    barrier()
+    clk = clocks.stop() if clocks else None
+    stage_ms, stage_n = sim.profile_read()
+    sim.profile(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+
+    # roofline of the fused stage kernel
+    peaks, peak_src = measured_peaks()
+    launches = sum(stage_n)
+    kernel_ms = sum(stage_ms) / max(launches, 1)
+    bytes_per_launch = 10 * nf * 8 * cells / 3.0
+    achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        key = "mhd_fp64_" + args.mode
+        if key in tj:
+            traffic = tj[key]["dram_bytes_per_cell_per_launch"] * cells
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+            "kernel": "k_stage (fused RHS+RK3+BCON+CFL), mean of the 3 stage launches",
+            "algorithmic_bytes_per_launch": bytes_per_launch, "kernel_ms_per_launch": kernel_ms,
+            "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured" else "fallback 6650 GB/s",
+            "stage_ms_per_launch": [m / max(n, 1) for m, n in zip(stage_ms, stage_n)]}
+
+    # ---- end to end through the C-ABI with pinned host buffers ----------
+    shape = setup.shape
+    nfort = shape[0] * shape[1] * shape[2]
+    pinned_t = [torch.empty(nfort, dtype=torch.float64, pin_memory=True) for _ in range(2 * nf)]
+    hin = {}
+    hout = {}
+    for i, f in enumerate(mhd3d.FIELDS[:nf]):
+        a = pinned_t[i].numpy().reshape(shape, order="F")
+        a[...] = setup.state[f]
+        hin[f] = a
+        hout[f] = pinned_t[nf + i].numpy().reshape(shape, order="F")
+    e2e_steps = args.steps
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    wt0 = time.perf_counter()
+    f0.record(stream)
+    st = sim.lib.mhd3d_upload(sim.h, *[mhd3d._ptr(hin.get(f)) for f in mhd3d.FIELDS])
+    assert st == 0, st
+    for _ in range(e2e_steps):
+        r = sim.step(1)
+    st = sim.lib.mhd3d_download(sim.h, *[mhd3d._ptr(hout.get(f)) for f in mhd3d.FIELDS])
+    assert st == 0, st
+    f1.record(stream)
+    f1.synchronize()
+    wall_e2e = time.perf_counter() - wt0
+    ms_e2e = max(f0.elapsed_time(f1), wall_e2e * 1e3)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    state_bytes = nf * nfort * 8
+    e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / e2e_steps,
+           "d2h_bytes_per_step": state_bytes / e2e_steps + 40,
+           "sequence": f"mhd3d_upload (pinned) + {e2e_steps} x mhd3d_step(1) with DT/TIMC/TIMT/UMACH/NIT read back "
+                       f"+ mhd3d_download (pinned)",
+           "ms": ms_e2e}
+
+    # ---- CPU baseline (rank 0, N=1) --------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_run(args.cpu_steps, 1)
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: rotating MHD polytrope from the host mirror of STATIC/TUBE model 4/RAN2",
+                "config": {"workload": WORKLOAD_NAME, "grid": [w["npx"], w["npy"], w["npz"]],
+                           "mode": args.mode, "fields": nf,
+                           "l2": f"state {3 * nf * cells * 8 / 1e9:.1f} GB in HBM >> 126 MB L2, no flush needed",
+                           "parallelism": f"{world} independent replica(s), one per GPU, no collectives",
+                           "last_dt": res["dt"], "nit": res["nit"]},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 4 * args.steps, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -165,6 +165,29 @@ int mhd3d_cfl(void* handle, double* dt, double* umach);
 /* BCON (3dmhdsub.f:2639-2958) applied to the current state in place. */
 int mhd3d_bcon(void* handle);
 
+/*
+ * Stream control and asynchronous stepping (no counterpart in the
+ * reference; they let a host overlap its own work with the step, capture
+ * steps in a CUDA graph and time them on its own stream).
+ *
+ * mhd3d_set_stream: run all later work of the handle on stream (a
+ *   cudaStream_t passed as void*); NULL returns to the handle's own stream.
+ * mhd3d_step_async: enqueue nsteps steps and return without waiting.
+ * mhd3d_sync: wait for enqueued steps and report as mhd3d_step does.
+ */
+int mhd3d_set_stream(void* handle, void* stream);
+int mhd3d_step_async(void* handle, int32_t nsteps);
+int mhd3d_sync(void* handle, double* dt, double* timc, double* timt, double* umach, int32_t* nit);
+
+/*
+ * Kernel timing for diagnostics: with enable != 0 every RK3 stage kernel
+ * is bracketed by CUDA events on the stream it runs on.  mhd3d_profile_read
+ * (after mhd3d_sync) returns the summed milliseconds and launch counts of
+ * stages 1, 2, 3 since the last read, then clears them.
+ */
+int mhd3d_profile(void* handle, int32_t enable);
+int mhd3d_profile_read(void* handle, double stage_ms[3], int32_t launches[3]);
+
 /* Version string of the library. */
 const char* mhd3d_version(void);
 

@@ -120,18 +120,19 @@ def reference_available() -> bool:
 
 
 def run_reference(params, grid: dict, state: dict, nsteps: int, npey: int = 1, npez: int = 2,
-                  mode: int = 0, exe: str = REF_EXE, timeout: float = 3600.0) -> dict:
+                  mode: int = 0, exe: str = REF_EXE, timeout: float = 3600.0, warmup: int = 0) -> dict:
     """Run the translated reference on the given global state.
 
     mode 0: nsteps x STEP, returns the fields and DT/TIMC/TIMT/UMACH/NIT.
     mode 1: one FLUXES, returns the right-hand sides.
+    warmup steps run before the timed ones ("seconds" covers the nsteps only).
     """
     nfld = 8 if params.lmag else 5
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         with open(fin, "wb") as f:
             f.write(b"R3DI")
-            f.write(struct.pack("<5i", 1, npey, npez, nsteps, mode))
+            f.write(struct.pack("<6i", 2, npey, npez, nsteps, mode, warmup))
             f.write(bytes(params))
             for n in GRID_NAMES:
                 f.write(np.ascontiguousarray(grid[n], dtype=np.float64).tobytes())

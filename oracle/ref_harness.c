@@ -4,7 +4,7 @@
  *
  * Usage: ref3dmhd IN OUT
  *
- * IN holds: "R3DI", version, npey, npez, nsteps, mode, the mhd3d_params
+ * IN holds: "R3DI", version, npey, npez, nsteps, mode, [warmup, version>=2], the mhd3d_params
  * struct, the 14 global COMMON/AJACOBI+CPEN arrays and the global fields
  * (Fortran (NPX+2,NPY+2,NPZ+2), as the single-domain driver holds them
  * after COMMUNICATE).  The harness forks NPEY*NPEZ ranks, gives each the
@@ -229,10 +229,11 @@ int main(int argc, char** argv)
     FILE* f = fopen(argv[1], "rb");
     if (!f) { perror(argv[1]); return 2; }
     char magic[4];
-    int32_t hdr[5];
+    int32_t hdr[6] = {0};
     if (fread(magic, 1, 4, f) != 4 || memcmp(magic, "R3DI", 4)) { fprintf(stderr, "bad input\n"); return 2; }
     if (fread(hdr, sizeof(int32_t), 5, f) != 5) return 2;
-    const int npey = hdr[1], npez = hdr[2], nsteps = hdr[3], mode = hdr[4];
+    if (hdr[0] >= 2 && fread(hdr + 5, sizeof(int32_t), 1, f) != 1) return 2;
+    const int npey = hdr[1], npez = hdr[2], nsteps = hdr[3], mode = hdr[4], warmup = hdr[5];
     mhd3d_params P;
     if (fread(&P, sizeof(P), 1, f) != 1) return 2;
     const int NXg = P.npx + 2, NYg = P.npy + 2, NZg = P.npz + 2;
@@ -339,6 +340,8 @@ int main(int argc, char** argv)
                     memcpy(loc[a] + (size_t)NX * (j + (size_t)NY * k),
                            fin[a] + (size_t)NXg * ((j + joff) + (size_t)NYg * (k + koff)), sizeof(double) * NX);
         }
+        if (mode == 0)
+            for (int s = 0; s < warmup; ++s) sub_STEP();
         barrier();
         double t0 = now();
         if (mode == 0) {

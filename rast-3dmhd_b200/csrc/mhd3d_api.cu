@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
@@ -36,6 +37,14 @@ struct Handle {
     int ntx = 0, zlen = 0, nchunks = 0;
     bool dt_valid = false;
     int gparity = 0;           // host copy of Control::gparity
+    cudaStream_t own = nullptr;   // the handle's stream; st may be a caller's
+    // asynchronous stepping: state at the last sync and steps enqueued since
+    int nit_base = 0, cur_base = 0, pending = 0;
+    // per-stage event timing
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_stage;    // stage of each recorded pair
+    size_t ev_used = 0;
 };
 
 #define CK(x)                                                                                    \
@@ -195,7 +204,8 @@ int destroy(Handle* h)
     cudaFree(h->met);
     cudaFree(h->ctl);
     cudaFree(h->acc);
-    if (h->st) cudaStreamDestroy(h->st);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    if (h->own) cudaStreamDestroy(h->own);
     delete h;
     return MHD3D_OK;
 }
@@ -213,7 +223,8 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     *out = h;   // released by the caller if anything below fails
     h->p = *p;
     CK(cudaGetDevice(&h->dev));
-    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+    h->st = h->own;
     const int npx = p->npx, npy = p->npy, npz = p->npz;
     const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
     h->nf = p->lmag ? 8 : 5;
@@ -354,6 +365,8 @@ int upload(Handle* h, const double* const f[8])
     CK(cudaMemcpyAsync(h->ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->dt_valid = false;
+    h->cur_base = h->cur;
+    h->pending = 0;
     return MHD3D_OK;
 }
 
@@ -387,40 +400,71 @@ int initial_dt(Handle* h)
     return MHD3D_OK;
 }
 
-int step(Handle* h, int n, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
+int record_event(Handle* h, int stage)
+{
+    if (h->ev_used + 2 > h->ev_pool.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            h->ev_pool.push_back(e);
+        }
+    }
+    if (stage >= 0) h->ev_stage.push_back(stage);
+    CK(cudaEventRecord(h->ev_pool[h->ev_used++], h->st));
+    return MHD3D_OK;
+}
+
+int step_async(Handle* h, int n)
 {
     CK(cudaSetDevice(h->dev));
     if (n < 0) return MHD3D_ERR_ARG;
-    Control c0{};
-    CK(cudaMemcpyAsync(&c0, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    // every call starts with a clear stop flag; DT of the current state comes
-    // from the last stage-3 reduction, or from a fresh CFL pass after a change
+    // a call that starts from a synced state clears the stop flag; DT of the
+    // current state comes from the last stage-3 reduction, or from a fresh
+    // CFL pass after the state changed
     if (!h->dt_valid) {
         int st = initial_dt(h);
         if (st) return st;
-    } else {
+    } else if (h->pending == 0) {
         k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
         CK(cudaGetLastError());
     }
-    const int cur0 = h->cur;
-    int cur = cur0;
+    int cur = h->cur_base ^ (h->pending & 1);
     for (int s = 0; s < n; ++s) {
         for (int stg = 1; stg <= 3; ++stg) {
             StageArgs a = make_args(h);
             a.u_in = h->ubuf[cur];
             a.u_out = h->ubuf[cur ^ 1];
+            if (h->prof) {
+                int st = record_event(h, stg - 1);
+                if (st) return st;
+            }
             CK(launch_stage(h, stg, a));
+            if (h->prof) {
+                int st = record_event(h, -1);
+                if (st) return st;
+            }
             cur ^= 1;
         }
         k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 1);
         CK(cudaGetLastError());
+        h->pending += 1;
     }
+    h->cur = cur;
+    return MHD3D_OK;
+}
+
+int sync(Handle* h, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
+{
+    CK(cudaSetDevice(h->dev));
     Control c{};
     CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    const int ran = c.nit - c0.nit;
-    h->cur = cur0 ^ (ran & 1);
+    // steps after a stop returned at once: the state is where the last completed step left it
+    const int ran = c.nit - h->nit_base;
+    h->cur = h->cur_base ^ (ran & 1);
+    h->cur_base = h->cur;
+    h->nit_base = c.nit;
+    h->pending = 0;
     h->gparity = c.gparity;
     if (dt) *dt = c.last_dt;
     if (timc) *timc = c.timc;
@@ -430,9 +474,18 @@ int step(Handle* h, int n, double* dt, double* timc, double* timt, double* umach
     return c.stop ? c.status : MHD3D_OK;
 }
 
+// reconcile enqueued steps before an entry point that reads the state
+int settle(Handle* h)
+{
+    if (h->pending == 0) return MHD3D_OK;
+    int st = sync(h, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return (st == MHD3D_ERR_CUDA) ? st : MHD3D_OK;
+}
+
 int fluxes(Handle* h, double* const out[8])
 {
     CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
     if (!h->fout) CK(cudaMalloc(&h->fout, sizeof(double) * h->nf * h->fstride));
     StageArgs a = make_args(h);
     CK(launch_stage(h, 0, a));
@@ -482,6 +535,7 @@ int mhd3d_upload(void* handle, const double* ru, const double* rv, const double*
 {
     if (!handle) return MHD3D_ERR_ARG;
     const double* f[8] = {ru, rv, rw, tt, ro, bx, by, bz};
+    if (int st = settle(static_cast<Handle*>(handle))) return st;
     return upload(static_cast<Handle*>(handle), f);
 }
 
@@ -490,13 +544,67 @@ int mhd3d_download(void* handle, double* ru, double* rv, double* rw, double* tt,
 {
     if (!handle) return MHD3D_ERR_ARG;
     double* f[8] = {ru, rv, rw, tt, ro, bx, by, bz};
+    if (int st = settle(static_cast<Handle*>(handle))) return st;
     return download(static_cast<Handle*>(handle), f);
 }
 
 int mhd3d_step(void* handle, int32_t nsteps, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
 {
     if (!handle) return MHD3D_ERR_ARG;
-    return step(static_cast<Handle*>(handle), nsteps, dt, timc, timt, umach, nit);
+    Handle* h = static_cast<Handle*>(handle);
+    int st = step_async(h, nsteps);
+    if (st) return st;
+    return sync(h, dt, timc, timt, umach, nit);
+}
+
+int mhd3d_step_async(void* handle, int32_t nsteps)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    return step_async(static_cast<Handle*>(handle), nsteps);
+}
+
+int mhd3d_sync(void* handle, double* dt, double* timc, double* timt, double* umach, int32_t* nit)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    return sync(static_cast<Handle*>(handle), dt, timc, timt, umach, nit);
+}
+
+int mhd3d_set_stream(void* handle, void* stream)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    Handle* h = static_cast<Handle*>(handle);
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->st));
+    h->st = stream ? static_cast<cudaStream_t>(stream) : h->own;
+    return MHD3D_OK;
+}
+
+int mhd3d_profile(void* handle, int32_t enable)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    static_cast<Handle*>(handle)->prof = enable != 0;
+    return MHD3D_OK;
+}
+
+int mhd3d_profile_read(void* handle, double stage_ms[3], int32_t launches[3])
+{
+    if (!handle || !stage_ms || !launches) return MHD3D_ERR_ARG;
+    Handle* h = static_cast<Handle*>(handle);
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->st));
+    for (int i = 0; i < 3; ++i) {
+        stage_ms[i] = 0.0;
+        launches[i] = 0;
+    }
+    for (size_t q = 0; q < h->ev_stage.size(); ++q) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev_pool[2 * q], h->ev_pool[2 * q + 1]));
+        stage_ms[h->ev_stage[q]] += ms;
+        launches[h->ev_stage[q]] += 1;
+    }
+    h->ev_stage.clear();
+    h->ev_used = 0;
+    return MHD3D_OK;
 }
 
 int mhd3d_fluxes(void* handle, double* fu, double* fv, double* fw, double* fr, double* ft, double* ww1,
@@ -512,6 +620,7 @@ int mhd3d_cfl(void* handle, double* dt, double* umach)
     if (!handle) return MHD3D_ERR_ARG;
     Handle* h = static_cast<Handle*>(handle);
     CK(cudaSetDevice(h->dev));
+    if (int st0 = settle(h)) return st0;
     int st = initial_dt(h);
     if (st) return st;
     Control c{};
@@ -527,6 +636,7 @@ int mhd3d_bcon(void* handle)
     if (!handle) return MHD3D_ERR_ARG;
     Handle* h = static_cast<Handle*>(handle);
     CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
     StageArgs a = make_args(h);
     CK(h->p.mode == MHD3D_MODE_FAST ? fast::launch_bcon(a, h->st) : exact::launch_bcon(a, h->st));
     CK(cudaStreamSynchronize(h->st));

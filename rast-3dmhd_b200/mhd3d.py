@@ -103,6 +103,12 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_cfl.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.mhd3d_bcon.argtypes = [vp]
     lib.mhd3d_version.restype = C.c_char_p
+    lib.mhd3d_set_stream.argtypes = [vp, vp]
+    lib.mhd3d_step_async.argtypes = [vp, C.c_int32]
+    lib.mhd3d_sync.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    lib.mhd3d_profile.argtypes = [vp, C.c_int32]
+    lib.mhd3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     return lib
 
 
@@ -232,6 +238,38 @@ class GpuSim:
             raise Mhd3dError(st, "mhd3d_step")
         return {"status": st, "dt": dt.value, "timc": timc.value, "timt": timt.value,
                 "umach": umach.value, "nit": nit.value}
+
+    def set_stream(self, stream_handle: int | None):
+        st = self.lib.mhd3d_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None)
+        if st:
+            raise Mhd3dError(st, "mhd3d_set_stream")
+
+    def step_async(self, n: int = 1):
+        st = self.lib.mhd3d_step_async(self.h, n)
+        if st:
+            raise Mhd3dError(st, "mhd3d_step_async")
+
+    def sync(self, check: bool = True) -> dict:
+        dt, timc, timt, umach = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        nit = C.c_int32()
+        st = self.lib.mhd3d_sync(self.h, C.byref(dt), C.byref(timc), C.byref(timt), C.byref(umach), C.byref(nit))
+        if st and check:
+            raise Mhd3dError(st, "mhd3d_sync")
+        return {"status": st, "dt": dt.value, "timc": timc.value, "timt": timt.value,
+                "umach": umach.value, "nit": nit.value}
+
+    def profile(self, enable: bool = True):
+        st = self.lib.mhd3d_profile(self.h, 1 if enable else 0)
+        if st:
+            raise Mhd3dError(st, "mhd3d_profile")
+
+    def profile_read(self):
+        ms = (C.c_double * 3)()
+        n = (C.c_int32 * 3)()
+        st = self.lib.mhd3d_profile_read(self.h, ms, n)
+        if st:
+            raise Mhd3dError(st, "mhd3d_profile_read")
+        return list(ms), list(n)
 
     def fluxes(self) -> dict:
         shape = self.setup.shape
