@@ -22,6 +22,7 @@ generated from the reference is committed.
 """
 from __future__ import annotations
 
+import os
 import re
 from dataclasses import dataclass, field
 
@@ -366,6 +367,7 @@ class Translator:
         self.units: dict[str, list[Stmt]] = {}
         self.out_funcs: list[str] = []
         self.uid = 0
+        self.param_base = os.path.basename(param_file).upper()
         self._read_params(param_file)
         # names from INCLUDE 'mpif.h', provided by the harness
         for n in ("MPI_COMM_WORLD", "MPI_STATUS_SIZE", "MPI_DOUBLE_PRECISION", "MPI_FLOAT",
@@ -646,7 +648,7 @@ class Translator:
             kw = kw.group(0) if kw else ""
             if kw in ("DIMENSION", "COMMON", "LOGICAL", "INTEGER", "DATA", "SAVE", "PARAMETER",
                       "IMPLICIT", "CHARACTER", "EXTERNAL", "REAL*8") or u.startswith("INCLUDE"):
-                if u.startswith("INCLUDE") and "3DMHDPARAM" not in u and "MPIF.H" not in u:
+                if u.startswith("INCLUDE") and self.param_base not in u and "MPIF.H" not in u:
                     raise TranslateError(f"INCLUDE {u}")
                 continue
             if s.label is not None:
