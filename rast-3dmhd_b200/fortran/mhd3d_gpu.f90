@@ -1,0 +1,80 @@
+! mhd3d_gpu.f90 -- ISO_C_BINDING interface of the B200 time-step library
+! (include/mhd3d.h) for the reference's Fortran driver.
+!
+! The driver keeps its COMMON blocks and calls these routines in place of
+! CALL STEP (3dmhd.f:912); see INTEGRATION.md for the patch.  The derived
+! type mirrors struct mhd3d_params field for field.
+module mhd3d_gpu
+  use, intrinsic :: iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: MHD3D_OK = 0, MHD3D_ERR_ARG = 1, MHD3D_ERR_CUDA = 2, &
+       MHD3D_ERR_NONFINITE = 3, MHD3D_ERR_DT_SMALL = 4, MHD3D_ERR_NO_DEVICE = 5, &
+       MHD3D_ERR_TIMEOUT = 6, MHD3D_ERR_NOMEM = 7
+  integer(c_int), parameter :: MHD3D_MODE_EXACT = 0, MHD3D_MODE_FAST = 1
+
+  type, bind(C) :: mhd3d_params
+     integer(c_int32_t) :: npx, npy, npz
+     integer(c_int32_t) :: lmag, lrot
+     integer(c_int32_t) :: izcon, itcon, ibcon
+     integer(c_int32_t) :: mode, reserved0
+     real(c_double) :: c13, c23, c43
+     real(c_double) :: hx, h2x, hy, h2y, hz, h2z
+     real(c_double) :: gam1, gam2, gam3, zeta1, zeta2
+     real(c_double) :: cv, ocv, ore, re, repr, theta, grav, gamma, sf
+     real(c_double) :: omx, omz
+     real(c_double) :: orm, rm, obeta
+     real(c_double) :: tb, tp, tc, xp, yp, hh
+     real(c_double) :: timi, timc
+     real(c_double) :: dtmin
+  end type mhd3d_params
+
+  interface
+     integer(c_int) function mhd3d_create(p, exx, dxxdx, d2xxdx2, ddx, wyy, dyydy, d2yydy2, ddy, &
+          zee, dzzdz, d2zzdz2, ddz, rkapa, dkapa, handle) bind(C, name="mhd3d_create")
+       import :: c_int, c_double, c_ptr, mhd3d_params
+       type(mhd3d_params), intent(in) :: p
+       real(c_double), intent(in) :: exx(*), dxxdx(*), d2xxdx2(*), ddx(*)
+       real(c_double), intent(in) :: wyy(*), dyydy(*), d2yydy2(*), ddy(*)
+       real(c_double), intent(in) :: zee(*), dzzdz(*), d2zzdz2(*), ddz(*)
+       real(c_double), intent(in) :: rkapa(*), dkapa(*)
+       type(c_ptr), intent(out) :: handle
+     end function mhd3d_create
+
+     integer(c_int) function mhd3d_destroy(handle) bind(C, name="mhd3d_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+     end function mhd3d_destroy
+
+     integer(c_int) function mhd3d_upload(handle, ru, rv, rw, tt, ro, bx, by, bz) bind(C, name="mhd3d_upload")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: handle
+       real(c_double), intent(in) :: ru(*), rv(*), rw(*), tt(*), ro(*), bx(*), by(*), bz(*)
+     end function mhd3d_upload
+
+     integer(c_int) function mhd3d_download(handle, ru, rv, rw, tt, ro, bx, by, bz) bind(C, name="mhd3d_download")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: handle
+       real(c_double), intent(out) :: ru(*), rv(*), rw(*), tt(*), ro(*), bx(*), by(*), bz(*)
+     end function mhd3d_download
+
+     integer(c_int) function mhd3d_step(handle, nsteps, dt, timc, timt, umach, nit) bind(C, name="mhd3d_step")
+       import :: c_int, c_int32_t, c_double, c_ptr
+       type(c_ptr), value :: handle
+       integer(c_int32_t), value :: nsteps
+       real(c_double), intent(out) :: dt, timc, timt, umach
+       integer(c_int32_t), intent(out) :: nit
+     end function mhd3d_step
+
+     integer(c_int) function mhd3d_cfl(handle, dt, umach) bind(C, name="mhd3d_cfl")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: handle
+       real(c_double), intent(out) :: dt, umach
+     end function mhd3d_cfl
+
+     integer(c_int) function mhd3d_bcon(handle) bind(C, name="mhd3d_bcon")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+     end function mhd3d_bcon
+  end interface
+end module mhd3d_gpu
