@@ -188,6 +188,37 @@ int mhd3d_sync(void* handle, double* dt, double* timc, double* timt, double* uma
 int mhd3d_profile(void* handle, int32_t enable);
 int mhd3d_profile_read(void* handle, double stage_ms[3], int32_t launches[3]);
 
+/*
+ * CFL/Mach reduction that allocates nothing.  No counterpart in the
+ * reference: it serves hosts that cannot call cudaMalloc (device arrays
+ * declared statically by a Fortran or C code, a framework allocator that
+ * owns the device heap, a hard device-memory cap) and already hold the
+ * state in device memory.
+ *
+ * Inputs are device pointers: the fields as Fortran (NX,NY,NZ) arrays
+ * (bx/by/bz only with lmag), and DDX(NX), DDY(NY), DDZ(NZ), RKAPA(NZ).
+ * out is a device pointer to 3 doubles: DT = SF*MIN(limits), UMACH, and
+ * 1.0 if any limit was not finite (else 0.0), as STEP computes them
+ * (3dmhdsub.f:741-873) and as mhd3d_cfl returns them in the
+ * reference-rounding mode.  The work is enqueued on stream (a cudaStream_t,
+ * NULL for the default stream) and the call returns without waiting.
+ *
+ * Scratch: one file-scope __device__ array of MHD3D_NOALLOC_MAX_PLANES x 6
+ * 64-bit words (192 KiB), held by every GPU that loads the library until
+ * the process exits; npz above MHD3D_NOALLOC_MAX_PLANES returns
+ * MHD3D_ERR_ARG.  The first call on a device looks the array's device
+ * address up on that device, so make that first call before any CUDA graph
+ * capture.  All calls share the array and keep the last call's contents:
+ * calls that can overlap on the GPU (different streams, or devices sharing
+ * a context) race and must be ordered by the caller.
+ */
+#define MHD3D_NOALLOC_MAX_PLANES 4096
+int mhd3d_cfl_noalloc(const mhd3d_params* p,
+                      const double* ru, const double* rv, const double* rw, const double* tt,
+                      const double* ro, const double* bx, const double* by, const double* bz,
+                      const double* ddx, const double* ddy, const double* ddz, const double* rkapa,
+                      double* out, void* stream);
+
 /* Version string of the library. */
 const char* mhd3d_version(void);
 

@@ -109,6 +109,7 @@ def gpu_lib() -> C.CDLL:
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     lib.mhd3d_profile.argtypes = [vp, C.c_int32]
     lib.mhd3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    lib.mhd3d_cfl_noalloc.argtypes = [C.POINTER(Params)] + [vp] * 13 + [vp]
     return lib
 
 
