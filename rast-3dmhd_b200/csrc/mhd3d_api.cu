@@ -20,13 +20,14 @@ struct Handle {
     mhd3d_params p;
     int dev = -1;
     cudaStream_t st = nullptr;
-    int nf = 0, pitch = 0;
-    size_t pstride = 0, fstride = 0;
+    int nf = 0;
+    int upitch = 0, urows = 0, zpitch = 0, zrows = 0;
+    size_t uf = 0, uz = 0, zf = 0, zz = 0;
     double* ubuf[2] = {nullptr, nullptr};
     int cur = 0;               // ubuf[cur] holds the current state
+    CUtensorMap map_u[2];      // TMA maps of the two U buffers
+    CUtensorMap map_z;
     double* z = nullptr;
-    double* ghost = nullptr;
-    double* gro = nullptr;
     double* stage = nullptr;   // one Fortran (NX,NY,NZ) field
     double* fout = nullptr;
     double* met = nullptr;     // all 1-D arrays, packed
@@ -57,42 +58,47 @@ struct Handle {
         }                                                                                        \
     } while (0)
 
-__global__ void k_unpack(const double* __restrict__ fort, double* __restrict__ u, double* __restrict__ g,
-                         int npx, int npy, int npz, int pitch, size_t pstride)
+__global__ void k_unpack(const double* __restrict__ fort, double* __restrict__ u0, double* __restrict__ u1,
+                         int npx, int npy, int npz, int upitch, size_t uz)
 {
-    // Fortran (NX,NY,NZ) -> interior planes of u and the two ghost planes of g
-    const int NX = npx + 2, NY = npy + 2;
-    const size_t n = (size_t)npx * npy * (npz + 2);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % npx), j = (int)((q / npx) % npy), K = (int)(q / ((size_t)npx * npy));
-        const double v = fort[(size_t)(i + 1) + (size_t)NX * ((size_t)(j + 1) + (size_t)NY * K)];
-        if (K == 0) g[(size_t)j * pitch + i] = v;
-        else if (K == npz + 1) g[(size_t)npy * pitch + (size_t)j * pitch + i] = v;
-        else u[(size_t)(K - 1) * pstride + (size_t)j * pitch + i] = v;
-    }
-}
-
-__global__ void k_pack(const double* __restrict__ u, const double* __restrict__ g, double* __restrict__ fort,
-                       int npx, int npy, int npz, int pitch, size_t pstride, int interior_only)
-{
-    // device layout -> Fortran (NX,NY,NZ) with the periodic halos COMMUNICATE leaves
+    // Fortran (NX,NY,NZ) -> both U buffers, halos refreshed from the interior
+    // (COMMUNICATE's periodic copies), ghost planes kept
     const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
     const size_t n = (size_t)NX * NY * NZ;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
         const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
-        if (interior_only) {
-            if (I == 0 || I == NX - 1 || J == 0 || J == NY - 1 || K == 0 || K == NZ - 1) {
-                fort[q] = 0.0;
-                continue;
-            }
-        }
-        int i = I - 1, j = J - 1;
-        i = i < 0 ? i + npx : (i >= npx ? i - npx : i);
-        j = j < 0 ? j + npy : (j >= npy ? j - npy : j);
-        double v;
-        if (K == 0) v = g[(size_t)j * pitch + i];
-        else if (K == NZ - 1) v = g[(size_t)npy * pitch + (size_t)j * pitch + i];
-        else v = u[(size_t)(K - 1) * pstride + (size_t)j * pitch + i];
+        const int Is = I == 0 ? npx : (I == NX - 1 ? 1 : I);
+        const int Js = J == 0 ? npy : (J == NY - 1 ? 1 : J);
+        const double v = fort[(size_t)Is + (size_t)NX * ((size_t)Js + (size_t)NY * K)];
+        const size_t d = (size_t)K * uz + (size_t)J * upitch + I;
+        u0[d] = v;
+        u1[d] = v;
+    }
+}
+
+__global__ void k_pack(const double* __restrict__ u, double* __restrict__ fort, int npx, int npy, int npz,
+                       int upitch, size_t uz)
+{
+    // U layout -> Fortran (NX,NY,NZ): the same index space, halos and ghost planes included
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        fort[q] = u[(size_t)K * uz + (size_t)J * upitch + I];
+    }
+}
+
+__global__ void k_pack_interior(const double* __restrict__ f, double* __restrict__ fort, int npx, int npy,
+                                int npz, int zpitch, size_t zz)
+{
+    // Z layout (interior cells) -> Fortran (NX,NY,NZ) with zeros outside the interior
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        double v = 0.0;
+        if (I > 0 && I < NX - 1 && J > 0 && J < NY - 1 && K > 0 && K < NZ - 1)
+            v = f[(size_t)(K - 1) * zz + (size_t)(J - 1) * zpitch + (I - 1)];
         fort[q] = v;
     }
 }
@@ -151,22 +157,53 @@ unsigned grid_for(size_t n)
 StageArgs make_args(Handle* h)
 {
     StageArgs a{};
+    a.map_u = h->map_u[h->cur];
+    a.map_z = h->map_z;
     a.u_in = h->ubuf[h->cur];
     a.u_out = h->ubuf[h->cur ^ 1];
     a.z = h->z;
     a.f_out = h->fout;
-    a.ghost = h->ghost;
-    a.gro = h->gro;
     a.ctl = h->ctl;
     a.acc = h->acc;
     a.m = h->m;
     a.s = h->s;
-    a.fstride = h->fstride;
-    a.pstride = h->pstride;
+    a.uf = h->uf;
+    a.uz = h->uz;
+    a.zf = h->zf;
+    a.zz = h->zz;
+    a.upitch = h->upitch;
+    a.zpitch = h->zpitch;
     a.ntx = h->ntx;
     a.zlen = h->zlen;
     a.nchunks = h->nchunks;
     return a;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 4-D tiled TMA map (x, y, z, field) of a double array, no swizzle, zero fill
+int make_map(CUtensorMap* map, double* base, const cuuint64_t dims[4], const cuuint32_t box[4])
+{
+    static EncodeTiledFn enc = nullptr;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+            return MHD3D_ERR_CUDA;
+        enc = reinterpret_cast<EncodeTiledFn>(fn);
+    }
+    const cuuint64_t strides[3] = {dims[0] * 8, dims[0] * dims[1] * 8, dims[0] * dims[1] * dims[2] * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        std::fprintf(stderr, "mhd3d: cuTensorMapEncodeTiled failed (%d)\n", (int)r);
+        return MHD3D_ERR_CUDA;
+    }
+    return MHD3D_OK;
 }
 
 cudaError_t launch_stage(Handle* h, int stage, const StageArgs& a)
@@ -197,8 +234,6 @@ int destroy(Handle* h)
     cudaFree(h->ubuf[0]);
     cudaFree(h->ubuf[1]);
     cudaFree(h->z);
-    cudaFree(h->ghost);
-    cudaFree(h->gro);
     cudaFree(h->stage);
     cudaFree(h->fout);
     cudaFree(h->met);
@@ -228,21 +263,38 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     const int npx = p->npx, npy = p->npy, npz = p->npz;
     const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
     h->nf = p->lmag ? 8 : 5;
-    h->pitch = (npx + 31) / 32 * 32;
-    h->pstride = (size_t)npy * h->pitch;
-    h->fstride = (size_t)npz * h->pstride;
-    const size_t ubytes = sizeof(double) * h->nf * h->fstride;
+    // U: the Fortran index space (halos, ghost planes), rows padded to even
+    // length and to at least one TMA box; Z: interior cells only
+    h->upitch = (NX + 1) / 2 * 2;
+    if (h->upitch < BW) h->upitch = BW;
+    h->urows = NY < BH ? BH : NY;
+    h->uz = (size_t)h->urows * h->upitch;
+    h->uf = (size_t)NZ * h->uz;
+    h->zpitch = (npx + 1) / 2 * 2;
+    if (h->zpitch < TX) h->zpitch = TX;
+    h->zrows = npy < TY ? TY : npy;
+    h->zz = (size_t)h->zrows * h->zpitch;
+    h->zf = (size_t)npz * h->zz;
+    const size_t ubytes = sizeof(double) * h->nf * h->uf;
+    const size_t zbytes = sizeof(double) * h->nf * h->zf;
     CK(cudaMalloc(&h->ubuf[0], ubytes));
     CK(cudaMalloc(&h->ubuf[1], ubytes));
-    CK(cudaMalloc(&h->z, ubytes));
+    CK(cudaMalloc(&h->z, zbytes));
     CK(cudaMemset(h->ubuf[0], 0, ubytes));
     CK(cudaMemset(h->ubuf[1], 0, ubytes));
-    CK(cudaMemset(h->z, 0, ubytes));
-    const size_t gplane = (size_t)npy * h->pitch;
-    CK(cudaMalloc(&h->ghost, sizeof(double) * 8 * 2 * gplane));
-    CK(cudaMemset(h->ghost, 0, sizeof(double) * 8 * 2 * gplane));
-    CK(cudaMalloc(&h->gro, sizeof(double) * 2 * 2 * gplane));
-    CK(cudaMemset(h->gro, 0, sizeof(double) * 2 * 2 * gplane));
+    CK(cudaMemset(h->z, 0, zbytes));
+    {
+        const cuuint64_t du[4] = {(cuuint64_t)h->upitch, (cuuint64_t)h->urows, (cuuint64_t)NZ, (cuuint64_t)h->nf};
+        const cuuint32_t bu[4] = {BW, BH, 1, (cuuint32_t)h->nf};
+        for (int b = 0; b < 2; ++b) {
+            int st2 = make_map(&h->map_u[b], h->ubuf[b], du, bu);
+            if (st2) return st2;
+        }
+        const cuuint64_t dz[4] = {(cuuint64_t)h->zpitch, (cuuint64_t)h->zrows, (cuuint64_t)npz, (cuuint64_t)h->nf};
+        const cuuint32_t bz[4] = {TX, TY, 1, (cuuint32_t)h->nf};
+        int st3 = make_map(&h->map_z, h->z, dz, bz);
+        if (st3) return st3;
+    }
     CK(cudaMalloc(&h->stage, sizeof(double) * (size_t)NX * NY * NZ));
     CK(cudaMalloc(&h->ctl, sizeof(Control)));
     CK(cudaMalloc(&h->acc, sizeof(Accum)));
@@ -316,7 +368,7 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     s.bot_flux = p->c23 * bot_dz * p->theta / src[9][NZ - 2];
     s.dtmin = p->dtmin;
     s.timi = p->timi;
-    s.npx = npx; s.npy = npy; s.npz = npz; s.pitch = h->pitch;
+    s.npx = npx; s.npy = npy; s.npz = npz; s.pitch = h->upitch;
     s.lmag = p->lmag; s.lrot = p->lrot; s.izcon = p->izcon; s.itcon = p->itcon; s.ibcon = p->ibcon;
     s.plume = plume;
     std::free(hm);
@@ -346,23 +398,14 @@ int upload(Handle* h, const double* const f[8])
     CK(cudaSetDevice(h->dev));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
-    const size_t gplane = (size_t)npy * h->pitch;
     for (int i = 0; i < h->nf; ++i)
         if (!f[i]) return MHD3D_ERR_ARG;
     for (int fi = 0; fi < h->nf; ++fi) {
         CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyHostToDevice, h->st));
-        double* g = (fi == F_RO) ? h->gro : h->ghost + (size_t)fi * 2 * gplane;
-        k_unpack<<<grid_for((size_t)npx * npy * (npz + 2)), 256, 0, h->st>>>(
-            h->stage, h->ubuf[h->cur] + (size_t)fi * h->fstride, g, npx, npy, npz, h->pitch, h->pstride);
+        k_unpack<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, h->ubuf[0] + (size_t)fi * h->uf,
+                                                     h->ubuf[1] + (size_t)fi * h->uf, npx, npy, npz, h->upitch, h->uz);
         CK(cudaGetLastError());
     }
-    // the uploaded RO ghost planes are the current copy
-    Control c{};
-    CK(cudaMemcpyAsync(&c, h->ctl, sizeof(Control), cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    c.gparity = 0;
-    h->gparity = 0;
-    CK(cudaMemcpyAsync(h->ctl, &c, sizeof(Control), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->dt_valid = false;
     h->cur_base = h->cur;
@@ -375,12 +418,10 @@ int download(Handle* h, double* const f[8])
     CK(cudaSetDevice(h->dev));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
-    const size_t gplane = (size_t)npy * h->pitch;
     for (int fi = 0; fi < h->nf; ++fi) {
         if (!f[fi]) continue;
-        const double* g = (fi == F_RO) ? h->gro + (size_t)h->gparity * 2 * gplane : h->ghost + (size_t)fi * 2 * gplane;
-        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->fstride, g, h->stage, npx, npy,
-                                                    npz, h->pitch, h->pstride, 0);
+        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->uf, h->stage, npx, npy, npz,
+                                                   h->upitch, h->uz);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
     }
@@ -432,6 +473,7 @@ int step_async(Handle* h, int n)
     for (int s = 0; s < n; ++s) {
         for (int stg = 1; stg <= 3; ++stg) {
             StageArgs a = make_args(h);
+            a.map_u = h->map_u[cur];
             a.u_in = h->ubuf[cur];
             a.u_out = h->ubuf[cur ^ 1];
             if (h->prof) {
@@ -486,15 +528,15 @@ int fluxes(Handle* h, double* const out[8])
 {
     CK(cudaSetDevice(h->dev));
     if (int st = settle(h)) return st;
-    if (!h->fout) CK(cudaMalloc(&h->fout, sizeof(double) * h->nf * h->fstride));
+    if (!h->fout) CK(cudaMalloc(&h->fout, sizeof(double) * h->nf * h->zf));
     StageArgs a = make_args(h);
     CK(launch_stage(h, 0, a));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
     for (int fi = 0; fi < h->nf; ++fi) {
         if (!out[fi]) continue;
-        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->fout + (size_t)fi * h->fstride, h->ghost, h->stage, npx, npy,
-                                                    npz, h->pitch, h->pstride, 1);
+        k_pack_interior<<<grid_for(nfort), 256, 0, h->st>>>(h->fout + (size_t)fi * h->zf, h->stage, npx, npy, npz,
+                                                            h->zpitch, h->zz);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
     }

@@ -1,15 +1,17 @@
 // mhd3d_dev.cuh -- device-side data structures shared by the step kernels.
 //
 // Layout in HBM (one handle):
-//   U, U', Z : nf fields x npz planes x npy rows x pitch doubles, interior
-//              cells only (Fortran I=2..NX-1, J=2..NY-1, K=2..NZ-1 map to
-//              i=I-2, j=J-2, k=K-2).  Field-major, x fastest.  The periodic
-//              x/y halos of the reference are not stored: every load wraps.
-//   ghost    : the reference's z ghost planes K=1 and K=NZ for RU,RV,RW,TT,
-//              BX,BY,BZ (never refreshed by the reference).
-//   gro      : two copies of the RO ghost planes; FLUXES inverts RO there on
-//              every call (3dmhdsub.f:1386-1391), the copies ping-pong.
+//   U, U' (ping-pong): nf fields x (NPZ+2) planes x (NPY+2) rows x upitch
+//              doubles, exactly the reference's (NX,NY,NZ) index space: the
+//              periodic x/y halo at index 0 and NPX+1 / NPY+1, the z ghost
+//              planes at 0 and NPZ+1 (never refreshed by the reference except
+//              RO, which FLUXES inverts there on every call, 3dmhdsub.f:1386-1391
+//              -- the two U buffers carry the two values).  upitch = NPX+2
+//              rounded up to even, so every row starts on 16 bytes and a tile
+//              with its halo is one in-bounds TMA box.  Field-major, x fastest.
+//   Z        : nf fields x NPZ x NPY x zpitch, interior cells only.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -21,8 +23,9 @@ namespace mhd3d {
 constexpr int TX = 32;            // tile width (one warp per row)
 constexpr int TY = 8;             // tile rows
 constexpr int NT = TX * TY;       // threads per CTA
-constexpr int SX = TX + 2;        // shared-memory row incl. periodic halo
-constexpr int SY = TY + 2;
+constexpr int BW = TX + 2;        // TMA box row: x0-1 .. x0+TX
+constexpr int BH = TY + 2;        // TMA box rows: y0-1 .. y0+TY
+constexpr int BSLOT = BW * BH;    // doubles of one field in one plane box
 
 enum Field { F_RU = 0, F_RV, F_RW, F_TT, F_RO, F_BX, F_BY, F_BZ };
 
@@ -79,18 +82,19 @@ struct Metrics {
 };
 
 struct StageArgs {
+    CUtensorMap map_u;      // TMA map of the input U buffer (x, y, z, field)
+    CUtensorMap map_z;      // TMA map of Z (x, y, z, field)
     const double* u_in;     // current state
     double* u_out;          // next state (other ping-pong buffer)
     double* z;              // Z (read in stages 2,3; written in stages 1,2)
-    double* f_out;          // RHS output (RHS-only launch)
-    const double* ghost;    // [8][2][npy][pitch]
-    double* gro;            // [2 copies][2 planes][npy][pitch]
+    double* f_out;          // RHS output (RHS-only launch), Z layout
     Control* ctl;
     Accum* acc;
     Metrics m;
     Scalars s;
-    size_t fstride;         // doubles per field
-    size_t pstride;         // doubles per plane (npy*pitch)
+    size_t uf, uz;          // U: doubles per field, per plane
+    size_t zf, zz;          // Z: doubles per field, per plane
+    int upitch, zpitch;
     int ntx;                // tiles along x
     int zlen;               // planes per z chunk
     int nchunks;
@@ -114,11 +118,13 @@ __host__ __device__ inline double of_key(unsigned long long k)
 // Launchers, one set per arithmetic mode (compiled from the same source
 // with and without FMA contraction).
 namespace exact {
+size_t stage_smem_bytes(int lmag);
 cudaError_t launch_stage(int stage, const StageArgs& a, cudaStream_t st);
 cudaError_t launch_cfl(const StageArgs& a, cudaStream_t st);
 cudaError_t launch_bcon(const StageArgs& a, cudaStream_t st);
 }
 namespace fast {
+size_t stage_smem_bytes(int lmag);
 cudaError_t launch_stage(int stage, const StageArgs& a, cudaStream_t st);
 cudaError_t launch_cfl(const StageArgs& a, cudaStream_t st);
 cudaError_t launch_bcon(const StageArgs& a, cudaStream_t st);

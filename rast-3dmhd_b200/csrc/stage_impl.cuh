@@ -7,15 +7,21 @@
 // the namespace of each copy.
 //
 // Work decomposition: a CTA owns a TX x TY tile of (x,y) columns and a
-// chunk of z planes and marches down the chunk.  Planes k-1, k, k+1 of the
-// prognostic fields plus the quantities FLUXES derives on the whole array
-// (1/RO, UU,VV,WW, pressure) sit in a 3-slot shared-memory ring with a
-// one-cell periodic halo, so every right-hand-side term of FLUXES
-// (3dmhdsub.f:1249-2634), including the 19-point cross terms of the
-// viscous stress, reads shared memory only.  The wall planes take BCON
-// (2751-2955) in the same pass: the thread owning a column keeps the new
-// values of the two planes next to each wall in registers.
+// chunk of z planes and marches down the chunk.  The raw fields of each
+// plane arrive by TMA (cp.async.bulk.tensor, one 4-D box per plane: x with
+// the periodic halo, y with the halo, one plane, all fields) into a
+// four-slot ring two planes ahead of the plane being computed; 1/RO of
+// planes k-1, k, k+1 sits in a three-slot ring next to it.  Velocities and
+// pressure are formed where they are used, from the same two operands
+// FLUXES multiplies (3dmhdsub.f:1386-1425), so every right-hand-side term
+// (1249-2634), including the 19-point cross terms, reads shared memory.
+// The Z tile of the plane (stages 2, 3) arrives by its own TMA box while
+// the right-hand side is computed.  The wall planes take BCON (2751-2955)
+// in the same pass: the thread owning a column keeps the new values of the
+// two planes next to each wall in registers.  No TMA load uses cluster
+// multicast.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/mhd3d.h"
@@ -25,78 +31,101 @@
 namespace mhd3d {
 namespace MHD3D_NS {
 
-template <bool MAG>
-struct NQ_ {
-    static constexpr int value = MAG ? 13 : 10;
-};
-// shared-memory quantity slots
 enum Q { Q_RU = 0, Q_RV, Q_RW, Q_RO, Q_TT, Q_RI, Q_UU, Q_VV, Q_WW, Q_P, Q_BX, Q_BY, Q_BZ };
 
-__device__ __forceinline__ int wrapi(int v, int n)
+constexpr int NRAW = 4;   // raw-plane ring slots (planes k-1, k, k+1 in use, k+2 in flight)
+constexpr int NRI = 3;    // 1/RO ring slots (planes k-1, k, k+1)
+constexpr long WAIT_LIMIT = 1L << 22;   // bounded mbarrier polls (~seconds)
+
+template <bool MAG>
+struct Lay {
+    static constexpr int NF = MAG ? 8 : 5;
+    static constexpr int RAW_SLOT = (NF * BSLOT * 8 + 127) / 128 * 128 / 8;   // doubles, 128-B aligned
+    static constexpr int ZT = NF * TY * TX;                                   // Z tile doubles
+    static constexpr int RI_OFF = NRAW * RAW_SLOT;
+    static constexpr int Z_OFF = ((RI_OFF + NRI * BSLOT) * 8 + 127) / 128 * 128 / 8;
+    static constexpr int BAR_OFF = Z_OFF + ZT;           // 5 mbarriers (8 B each)
+    static constexpr int RED_OFF = BAR_OFF + 8;          // CFL block reduction
+    static constexpr int FLAG_OFF = RED_OFF + (NT / 32) * 6;
+    static constexpr int TOTAL = FLAG_OFF + 2;
+    static constexpr size_t BYTES = (size_t)TOTAL * 8 + 128;   // + alignment slack
+};
+
+// value of quantity QQ at offset off of a plane slot: raw fields, 1/RO, and the
+// products FLUXES forms on the whole array (UU=RU*RO' with RO'=1/RO, WW1=RO*TT)
+template <int QQ>
+__device__ __forceinline__ double qv(const double* __restrict__ raw, const double* __restrict__ ri, int off)
 {
-    v %= n;
-    return v < 0 ? v + n : v;
+    if constexpr (QQ == Q_RU) return raw[F_RU * BSLOT + off];
+    else if constexpr (QQ == Q_RV) return raw[F_RV * BSLOT + off];
+    else if constexpr (QQ == Q_RW) return raw[F_RW * BSLOT + off];
+    else if constexpr (QQ == Q_RO) return raw[F_RO * BSLOT + off];
+    else if constexpr (QQ == Q_TT) return raw[F_TT * BSLOT + off];
+    else if constexpr (QQ == Q_BX) return raw[F_BX * BSLOT + off];
+    else if constexpr (QQ == Q_BY) return raw[F_BY * BSLOT + off];
+    else if constexpr (QQ == Q_BZ) return raw[F_BZ * BSLOT + off];
+    else if constexpr (QQ == Q_RI) return ri[off];
+    else if constexpr (QQ == Q_UU) return raw[F_RU * BSLOT + off] * ri[off];
+    else if constexpr (QQ == Q_VV) return raw[F_RV * BSLOT + off] * ri[off];
+    else if constexpr (QQ == Q_WW) return raw[F_RW * BSLOT + off] * ri[off];
+    else return raw[F_RO * BSLOT + off] * raw[F_TT * BSLOT + off];
 }
 
-// Load plane kp (-1 and npz are the ghost planes) of the tile into ring slot.
-template <bool MAG>
-__device__ __forceinline__ void load_plane(const StageArgs& a, double* __restrict__ sm, int slot, int kp,
-                                           int x0, int y0, int rd)
+// ---- TMA and mbarrier primitives (PTX) ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned cnt)
 {
-    constexpr int NQ = NQ_<MAG>::value;
-    const int npx = a.s.npx, npy = a.s.npy, npz = a.s.npz, pitch = a.s.pitch;
-    double* base = sm + (size_t)slot * NQ * SX * SY;
-    for (int p = threadIdx.x; p < SX * SY; p += NT) {
-        const int lx = p % SX, ly = p / SX;
-        const int gx = wrapi(x0 - 1 + lx, npx), gy = wrapi(y0 - 1 + ly, npy);
-        double ru, rv, rw, ro, tt, bx = 0, by = 0, bz = 0;
-        if (kp >= 0 && kp < npz) {
-            const size_t c = (size_t)kp * a.pstride + (size_t)gy * pitch + gx;
-            ru = a.u_in[c + F_RU * a.fstride];
-            rv = a.u_in[c + F_RV * a.fstride];
-            rw = a.u_in[c + F_RW * a.fstride];
-            tt = a.u_in[c + F_TT * a.fstride];
-            ro = a.u_in[c + F_RO * a.fstride];
-            if (MAG) {
-                bx = a.u_in[c + F_BX * a.fstride];
-                by = a.u_in[c + F_BY * a.fstride];
-                bz = a.u_in[c + F_BZ * a.fstride];
-            }
-        } else {
-            const int g = kp < 0 ? 0 : 1;
-            const size_t gp = (size_t)npy * pitch;
-            const size_t c = (size_t)g * gp + (size_t)gy * pitch + gx;
-            ru = a.ghost[(size_t)F_RU * 2 * gp + c];
-            rv = a.ghost[(size_t)F_RV * 2 * gp + c];
-            rw = a.ghost[(size_t)F_RW * 2 * gp + c];
-            tt = a.ghost[(size_t)F_TT * 2 * gp + c];
-            ro = a.gro[(size_t)rd * 2 * gp + c];
-            if (MAG) {
-                bx = a.ghost[(size_t)F_BX * 2 * gp + c];
-                by = a.ghost[(size_t)F_BY * 2 * gp + c];
-                bz = a.ghost[(size_t)F_BZ * 2 * gp + c];
-            }
-        }
-        // loops 90 and 160-180 of FLUXES: pressure from rho, then 1/rho and u=rho*u*(1/rho)
-        const double pr = ro * tt;
-        const double ri = 1.0 / ro;
-        double* q = base + ly * SX + lx;
-        q[Q_RU * SX * SY] = ru;
-        q[Q_RV * SX * SY] = rv;
-        q[Q_RW * SX * SY] = rw;
-        q[Q_RO * SX * SY] = ro;
-        q[Q_TT * SX * SY] = tt;
-        q[Q_RI * SX * SY] = ri;
-        q[Q_UU * SX * SY] = ru * ri;
-        q[Q_VV * SX * SY] = rv * ri;
-        q[Q_WW * SX * SY] = rw * ri;
-        q[Q_P * SX * SY] = pr;
-        if (MAG) {
-            q[Q_BX * SX * SY] = bx;
-            q[Q_BY * SX * SY] = by;
-            q[Q_BZ * SX * SY] = bz;
-        }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(cnt) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase with the given parity; false when it gave up
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    for (long it = 0; it < WAIT_LIMIT; ++it) {
+        if (mbar_test(bar, parity)) return true;
+        if (it > 32) __nanosleep(128);
     }
+    return false;
+}
+__device__ __forceinline__ void tma_load4(void* dst, const CUtensorMap* map, unsigned long long* bar, int x, int y,
+                                          int z, int f)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(f),
+          "r"(smem_u32(bar))
+        : "memory");
+}
+
+// store a cell of U and the periodic halo copies COMMUNICATE would make of it
+__device__ __forceinline__ void store_u(double* __restrict__ u, size_t fofs, const StageArgs& a, int gi, int gj,
+                                        int kz, double v)
+{
+    const int npx = a.s.npx, npy = a.s.npy;
+    const size_t base = fofs + (size_t)kz * a.uz;
+    const int ix = gi + 1, jy = gj + 1;
+    u[base + (size_t)jy * a.upitch + ix] = v;
+    const int hx = (gi == 0) ? npx + 1 : (gi == npx - 1) ? 0 : -1;
+    const int hy = (gj == 0) ? npy + 1 : (gj == npy - 1) ? 0 : -1;
+    if (hx >= 0) u[base + (size_t)jy * a.upitch + hx] = v;
+    if (hy >= 0) u[base + (size_t)hy * a.upitch + ix] = v;
+    if (hx >= 0 && hy >= 0) u[base + (size_t)hy * a.upitch + hx] = v;
 }
 
 // Block-wide reduction of the CFL parts into the global accumulators.
@@ -146,17 +175,27 @@ __device__ __forceinline__ void cfl_commit(Accum* acc, unsigned long long k1, un
 // STAGE 1..3: the RK3 substeps of STEP (3dmhdsub.f:874-1169).
 // ---------------------------------------------------------------------------
 template <bool MAG, bool ROT, int STAGE>
-__global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
+__global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageArgs a)
 {
-    constexpr int NQ = NQ_<MAG>::value;
-    extern __shared__ double sm[];
+    using L = Lay<MAG>;
+    constexpr int NF = L::NF;
+    extern __shared__ unsigned char smem_raw[];
+    double* const sbase = reinterpret_cast<double*>((reinterpret_cast<size_t>(smem_raw) + 127) & ~(size_t)127);
+    double* const sraw = sbase;
+    double* const sri = sbase + L::RI_OFF;
+    double* const sz = sbase + L::Z_OFF;
+    unsigned long long* const bars = reinterpret_cast<unsigned long long*>(sbase + L::BAR_OFF);
+    unsigned long long* const red = reinterpret_cast<unsigned long long*>(sbase + L::RED_OFF);
+    int* const sflag = reinterpret_cast<int*>(sbase + L::FLAG_OFF);
+
     const Control* ctl = a.ctl;
     if (STAGE != 0 && ctl->stop) return;
 
     const Scalars& s = a.s;
     const Metrics& m = a.m;
-    const int npx = s.npx, npy = s.npy, npz = s.npz, pitch = s.pitch;
-    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const int npx = s.npx, npy = s.npy, npz = s.npz;
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
     const int tile = blockIdx.x;
     const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
     const int chunk = blockIdx.y;
@@ -166,44 +205,99 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
     const bool active = gi < npx && gj < npy;
     const int lx = tx + 1, ly = ty + 1;
 
-    // ghost RO copy read by this FLUXES call and the one it leaves behind
-    const int rd = (STAGE == 0) ? ctl->gparity : ((ctl->gparity + STAGE - 1) & 1);
-    const int wr = rd ^ 1;
-
     const double DT = ctl->dt;
     const double cu = STAGE == 1 ? s.gam1 * DT : STAGE == 2 ? s.gam2 * DT : s.gam3 * DT;   // COEF for U
     const double cz = STAGE == 1 ? s.zeta1 * DT : s.zeta2 * DT;                            // COEF for Z
 
-    // tile column metrics
     const double dxi = active ? m.dxxdx[gi + 1] : 0.0, d2xi = active ? m.d2xxdx2[gi + 1] : 0.0;
     const double dyj = active ? m.dyydy[gj + 1] : 0.0, d2yj = active ? m.d2yydy2[gj + 1] : 0.0;
     const double HX = s.hx, H2X = s.h2x, HY = s.hy, H2Y = s.h2y, HZ = s.hz, H2Z = s.h2z;
     const double C13 = s.c13, C23 = s.c23, C43 = s.c43, OCV = s.ocv, ORE = s.ore;
 
-    // history of new values for BCON (RU, RV, RO, TT) at k-1 and k-2
-    double h1_ru = 0, h1_rv = 0, h1_ro = 0, h1_tt = 0, h2_ru = 0, h2_rv = 0, h2_ro = 0, h2_tt = 0;
-    // new values of the top wall kept until planes 1 and 2 are done
-    double w0_ro = 0, w0_bx = 0, w0_by = 0, w0_bz = 0, w0_tt = 0;
-    // CFL accumulation (stage 3)
     unsigned long long kw1 = ~0ull, kw2 = ~0ull, kw3 = ~0ull, kw4 = ~0ull, kmu = 0ull;
     unsigned int bad = 0;
 
-    const size_t gp = (size_t)npy * pitch;
-    const size_t col = (size_t)gj * pitch + gi;
+    const unsigned raw_bytes = (unsigned)(NF * BSLOT * 8);
+    const unsigned z_bytes = (unsigned)(NF * TY * TX * 8);
+    // own column in the U layout (periodic halo at index 0 and NPX+1 / NPY+1,
+    // ghost planes at 0 and NPZ+1) and in the compact Z/F layout
+    const size_t ucol = (size_t)(gj + 1) * a.upitch + (gi + 1);
+    const size_t zcol = (size_t)gj * a.zpitch + gi;
 
-    load_plane<MAG>(a, sm, (k0 - 1 + 3) % 3, k0 - 1, x0, y0, rd);
-    load_plane<MAG>(a, sm, k0 % 3, k0, x0, y0, rd);
+    if (tid == 0) {
+        for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
+        *sflag = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    // plane kp (-1 .. npz) lives in raw slot (kp+1)&3 and 1/RO slot (kp+1)%3;
+    // it is the ((kp-(k0-1))>>2)-th fill of its slot
+    int hi_issued = k0 - 2;   // thread 0: highest plane issued so far
+    auto issue_plane = [&](int kp) {
+        const int sl = (kp + 1) & 3;
+        fence_proxy_async();
+        mbar_expect_tx(&bars[sl], raw_bytes);
+        tma_load4(sraw + (size_t)sl * L::RAW_SLOT, &a.map_u, &bars[sl], x0, y0, kp + 1, 0);
+        hi_issued = kp;
+    };
+    auto parity_of = [&](int kp) -> unsigned { return (unsigned)(((kp - (k0 - 1)) >> 2) & 1); };
+    auto derive_ri = [&](int kp) {
+        const double* r = sraw + (size_t)((kp + 1) & 3) * L::RAW_SLOT + F_RO * BSLOT;
+        double* d = sri + (size_t)((kp + 1) % 3) * BSLOT;
+        for (int p = tid; p < BSLOT; p += NT) d[p] = 1.0 / r[p];
+    };
+
+    if (tid == 0)
+        for (int kp = k0 - 1; kp <= k0 + 2 && kp <= k1; ++kp) issue_plane(kp);
+    bool ok = mbar_wait(&bars[(k0 + 0) & 3], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) & 3], parity_of(k0));
+    if (ok) {
+        derive_ri(k0 - 1);
+        derive_ri(k0);
+    } else {
+        atomicOr(sflag, 1);
+    }
+    bool zpending = false;   // thread 0: a Z fill is in flight
+    int zfill = 0;           // fills of the Z barrier so far
 
     for (int k = k0; k < k1; ++k) {
-        load_plane<MAG>(a, sm, (k + 1) % 3, k + 1, x0, y0, rd);
+        if (STAGE >= 2 && tid == 0 && !*sflag) {
+            fence_proxy_async();
+            mbar_expect_tx(&bars[NRAW], z_bytes);
+            tma_load4(sz, &a.map_z, &bars[NRAW], x0, y0, k, 0);
+            zpending = true;
+        }
+        if (!mbar_wait(&bars[(k + 2) & 3], parity_of(k + 1))) atomicOr(sflag, 1);
+        else derive_ri(k + 1);
         __syncthreads();
+        if (*sflag) break;
+        bool zok = true;
         if (active) {
-            const double* Sm = sm + (size_t)((k + 2) % 3) * NQ * SX * SY;  // plane k-1
-            const double* Sc = sm + (size_t)(k % 3) * NQ * SX * SY;        // plane k
-            const double* Sp = sm + (size_t)((k + 1) % 3) * NQ * SX * SY;  // plane k+1
-#define C_(q, dx, dy) Sc[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
-#define M_(q, dx, dy) Sm[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
-#define P_(q, dx, dy) Sp[(q) * SX * SY + (ly + (dy)) * SX + (lx + (dx))]
+            const double* Rm = sraw + (size_t)((k + 0) & 3) * L::RAW_SLOT;   // plane k-1
+            const double* Rc = sraw + (size_t)((k + 1) & 3) * L::RAW_SLOT;   // plane k
+            const double* Rp = sraw + (size_t)((k + 2) & 3) * L::RAW_SLOT;   // plane k+1
+            const double* Im = sri + (size_t)((k + 0) % 3) * BSLOT;
+            const double* Ic = sri + (size_t)((k + 1) % 3) * BSLOT;
+            const double* Ip = sri + (size_t)((k + 2) % 3) * BSLOT;
+#define C_(q, dx, dy) qv<q>(Rc, Ic, (ly + (dy)) * BW + (lx + (dx)))
+#define M_(q, dx, dy) qv<q>(Rm, Im, (ly + (dy)) * BW + (lx + (dx)))
+#define P_(q, dx, dy) qv<q>(Rp, Ip, (ly + (dy)) * BW + (lx + (dx)))
+#define WALL_LOADS                                                                                   \
+    double rw2 = 0, ww2 = 0, bx2 = 0, bx3 = 0, by2 = 0, by3 = 0;                                     \
+    if (top || bot) {                                                                                \
+        /* own column two and three planes inside the wall (one-sided stencils) */                  \
+        const int kk2 = top ? 2 : npz - 3, kk3 = top ? 3 : npz - 4;                                  \
+        const size_t c2 = (size_t)(kk2 + 1) * a.uz + ucol, c3 = (size_t)(kk3 + 1) * a.uz + ucol;     \
+        rw2 = a.u_in[c2 + F_RW * a.uf];                                                              \
+        const double ro2 = a.u_in[c2 + F_RO * a.uf];                                                 \
+        ww2 = rw2 * (1.0 / ro2);                                                                     \
+        if (MAG) {                                                                                   \
+            bx2 = a.u_in[c2 + F_BX * a.uf];                                                          \
+            bx3 = a.u_in[c3 + F_BX * a.uf];                                                          \
+            by2 = a.u_in[c2 + F_BY * a.uf];                                                          \
+            by3 = a.u_in[c3 + F_BY * a.uf];                                                          \
+        }                                                                                            \
+    }
             const bool top = (k == 0), bot = (k == npz - 1);
             const double dzk = m.dzzdz[k + 1], d2zk = m.d2zzdz2[k + 1];
             const double rka = m.rkapa[k + 1], dka = m.dkapa[k + 1];
@@ -211,21 +305,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
             const double tmpz1 = HZ * d2zk, tmpz2 = H2Z * dzk * dzk;
             const double tmpy1 = HY * d2yj, tmpy2 = H2Y * dyj * dyj;
 
-            // own-column values two and three planes inside a wall (one-sided stencils)
-            double rw2 = 0, ww2 = 0, bx2 = 0, bx3 = 0, by2 = 0, by3 = 0;
-            if (top || bot) {
-                const int kk2 = top ? 2 : npz - 3, kk3 = top ? 3 : npz - 4;
-                const size_t c2 = (size_t)kk2 * a.pstride + col, c3 = (size_t)kk3 * a.pstride + col;
-                rw2 = a.u_in[c2 + F_RW * a.fstride];
-                const double ro2 = a.u_in[c2 + F_RO * a.fstride];
-                ww2 = rw2 * (1.0 / ro2);
-                if (MAG) {
-                    bx2 = a.u_in[c2 + F_BX * a.fstride];
-                    bx3 = a.u_in[c3 + F_BX * a.fstride];
-                    by2 = a.u_in[c2 + F_BY * a.fstride];
-                    by3 = a.u_in[c3 + F_BY * a.fstride];
-                }
-            }
+            WALL_LOADS
 
             const double RUc = C_(Q_RU, 0, 0), RVc = C_(Q_RV, 0, 0), RWc = C_(Q_RW, 0, 0);
             const double ROc = C_(Q_RO, 0, 0), TTc = C_(Q_TT, 0, 0), RIc = C_(Q_RI, 0, 0);
@@ -419,25 +499,26 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
             }
             // ghost RO planes: this FLUXES call leaves 1/RO behind (3dmhdsub.f:1386-1391)
             if (STAGE != 0) {
-                if (top) a.gro[(size_t)wr * 2 * gp + col] = M_(Q_RI, 0, 0);
-                if (bot) a.gro[(size_t)wr * 2 * gp + gp + col] = P_(Q_RI, 0, 0);
+                if (top) store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, 0, M_(Q_RI, 0, 0));
+                if (bot) store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, npz + 1, P_(Q_RI, 0, 0));
             }
 #undef C_
 #undef M_
 #undef P_
-            const size_t c = (size_t)k * a.pstride + col;
+#undef WALL_LOADS
             const bool wall = top || bot;
+            const size_t zc = (size_t)k * a.zz + zcol;
             if (STAGE == 0) {
                 // right-hand sides; values BCON discards on the walls are reported as 0
-                a.f_out[c + 0 * a.fstride] = wall ? 0.0 : fu;
-                a.f_out[c + 1 * a.fstride] = wall ? 0.0 : fv;
-                a.f_out[c + 2 * a.fstride] = wall ? 0.0 : fw;
-                a.f_out[c + 3 * a.fstride] = fr;
-                a.f_out[c + 4 * a.fstride] = wall ? 0.0 : ft;
+                a.f_out[zc + 0 * a.zf] = wall ? 0.0 : fu;
+                a.f_out[zc + 1 * a.zf] = wall ? 0.0 : fv;
+                a.f_out[zc + 2 * a.zf] = wall ? 0.0 : fw;
+                a.f_out[zc + 3 * a.zf] = fr;
+                a.f_out[zc + 4 * a.zf] = wall ? 0.0 : ft;
                 if (MAG) {
-                    a.f_out[c + 5 * a.fstride] = w1;
-                    a.f_out[c + 6 * a.fstride] = w2;
-                    a.f_out[c + 7 * a.fstride] = wall ? 0.0 : w3;
+                    a.f_out[zc + 5 * a.zf] = w1;
+                    a.f_out[zc + 6 * a.zf] = w2;
+                    a.f_out[zc + 7 * a.zf] = wall ? 0.0 : w3;
                 }
             } else {
                 // ---- RK3 update: U = Z + COEF*F (STEP loops 70-140, 270-340, 470-540);
@@ -447,54 +528,55 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
                     zu = RUc; zv = RVc; zw = RWc; zr = ROc; zt = TTc;
                     if (MAG) { zbx = BXc0; zby = BYc0; zbz = BZc0; }
                 } else {
-                    zu = a.z[c + F_RU * a.fstride];
-                    zv = a.z[c + F_RV * a.fstride];
-                    zw = a.z[c + F_RW * a.fstride];
-                    zt = a.z[c + F_TT * a.fstride];
-                    zr = a.z[c + F_RO * a.fstride];
+                    zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
+                    const double* zt_ = sz + ty * TX + tx;
+                    zu = zt_[F_RU * TY * TX];
+                    zv = zt_[F_RV * TY * TX];
+                    zw = zt_[F_RW * TY * TX];
+                    zt = zt_[F_TT * TY * TX];
+                    zr = zt_[F_RO * TY * TX];
                     if (MAG) {
-                        zbx = a.z[c + F_BX * a.fstride];
-                        zby = a.z[c + F_BY * a.fstride];
-                        zbz = a.z[c + F_BZ * a.fstride];
+                        zbx = zt_[F_BX * TY * TX];
+                        zby = zt_[F_BY * TY * TX];
+                        zbz = zt_[F_BZ * TY * TX];
                     }
                 }
                 const double nu = zu + cu * fu, nv = zv + cu * fv, nw = zw + cu * fw;
                 const double nr = zr + cu * fr, nt = zt + cu * ft;
                 const double nbx = zbx + cu * w1, nby = zby + cu * w2, nbz = zbz + cu * w3;
-                double* uo = a.u_out + c;
-                uo[F_RO * a.fstride] = nr;
-                if (MAG) {
-                    uo[F_BX * a.fstride] = nbx;
-                    uo[F_BY * a.fstride] = nby;
-                }
-                if (!wall) {
-                    uo[F_RU * a.fstride] = nu;
-                    uo[F_RV * a.fstride] = nv;
-                    uo[F_RW * a.fstride] = nw;
-                    uo[F_TT * a.fstride] = nt;
-                    if (MAG) uo[F_BZ * a.fstride] = nbz;
-                }
-                // ---- Z for the next stage: Z = U + ZETA*DT*F (loops 190-260, 390-460).
-                //      On the walls only RO, BX, BY are ever read back.
-                if (STAGE < 3) {
-                    double* zo = a.z + c;
-                    zo[F_RO * a.fstride] = nr + cz * fr;
+                const int kz = k + 1;
+                if (zok) {
+                    store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, kz, nr);
                     if (MAG) {
-                        zo[F_BX * a.fstride] = nbx + cz * w1;
-                        zo[F_BY * a.fstride] = nby + cz * w2;
+                        store_u(a.u_out, (size_t)F_BX * a.uf, a, gi, gj, kz, nbx);
+                        store_u(a.u_out, (size_t)F_BY * a.uf, a, gi, gj, kz, nby);
                     }
-                    if (!wall) {
-                        zo[F_RU * a.fstride] = nu + cz * fu;
-                        zo[F_RV * a.fstride] = nv + cz * fv;
-                        zo[F_RW * a.fstride] = nw + cz * fw;
-                        zo[F_TT * a.fstride] = nt + cz * ft;
-                        if (MAG) zo[F_BZ * a.fstride] = nbz + cz * w3;
+                    // on the walls RU, RV, RW, TT, BZ are rewritten by BCON below
+                    store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, kz, nu);
+                    store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, kz, nv);
+                    store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, kz, nw);
+                    store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, kz, nt);
+                    if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, kz, nbz);
+                    // ---- Z for the next stage: Z = U + ZETA*DT*F (loops 190-260, 390-460).
+                    //      On the walls only RO, BX, BY are ever read back.
+                    if (STAGE < 3) {
+                        double* zo = a.z + zc;
+                        zo[F_RO * a.zf] = nr + cz * fr;
+                        if (MAG) {
+                            zo[F_BX * a.zf] = nbx + cz * w1;
+                            zo[F_BY * a.zf] = nby + cz * w2;
+                        }
+                        if (!wall) {
+                            zo[F_RU * a.zf] = nu + cz * fu;
+                            zo[F_RV * a.zf] = nv + cz * fv;
+                            zo[F_RW * a.zf] = nw + cz * fw;
+                            zo[F_TT * a.zf] = nt + cz * ft;
+                            if (MAG) zo[F_BZ * a.zf] = nbz + cz * w3;
+                        }
                     }
                 }
                 // ---- BCON (3dmhdsub.f:2751-2955) and the CFL parts of the next step
-                if (top) {
-                    w0_ro = nr; w0_bx = nbx; w0_by = nby; w0_bz = nbz; w0_tt = nt;
-                } else if (!bot) {
+                if (!top && !bot) {
                     if (STAGE == 3) {
                         CflPart cp;
                         cfl_cell<MAG>(s, nu, nv, nw, nr, nt, nbx, nby, nbz, cell_dd(m, gi, gj, k), rka, cp);
@@ -504,7 +586,15 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
                     }
                 }
                 if (k == 2 && k0 == 0) {
-                    // top wall: new values of planes K=3 (h1) and K=4 (this plane)
+                    // top wall: new values of planes K=3 (read back) and K=4 (this plane);
+                    // this thread wrote planes K=2 and K=3 of u_out itself
+                    const double* ub = a.u_out + ucol;
+                    const size_t c0 = 1 * a.uz, c1 = 2 * a.uz;
+                    const double h1_ru = ub[F_RU * a.uf + c1], h1_rv = ub[F_RV * a.uf + c1];
+                    const double h1_ro = ub[F_RO * a.uf + c1], h1_tt = ub[F_TT * a.uf + c1];
+                    const double w0_ro = ub[F_RO * a.uf + c0], w0_tt = ub[F_TT * a.uf + c0];
+                    const double w0_bx = MAG ? ub[F_BX * a.uf + c0] : 0.0, w0_by = MAG ? ub[F_BY * a.uf + c0] : 0.0;
+                    const double w0_bz = MAG ? ub[F_BZ * a.uf + c0] : 0.0;
                     const double ru_w = w0_ro * (C43 * h1_ru / h1_ro - C13 * nu / nr);
                     const double rv_w = w0_ro * (C43 * h1_rv / h1_ro - C13 * nv / nr);
                     double tt_w = w0_tt;
@@ -520,13 +610,13 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
                         tt_w = C43 * h1_tt - C13 * nt - s.top_flux;
                     }
                     const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : w0_bz;
-                    const size_t c0 = col;
-                    double* u0 = a.u_out + c0;
-                    u0[F_RU * a.fstride] = ru_w;
-                    u0[F_RV * a.fstride] = rv_w;
-                    u0[F_RW * a.fstride] = 0.0;
-                    u0[F_TT * a.fstride] = tt_w;
-                    if (MAG) u0[F_BZ * a.fstride] = bz_w;
+                    if (zok) {
+                        store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, 1, ru_w);
+                        store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, 1, rv_w);
+                        store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, 1, 0.0);
+                        store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, 1, tt_w);
+                        if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, 1, bz_w);
+                    }
                     if (STAGE == 3) {
                         CflPart cp;
                         cfl_cell<MAG>(s, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w, cell_dd(m, gi, gj, 0),
@@ -537,16 +627,24 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
                     }
                 }
                 if (bot) {
-                    // bottom wall: new values of planes K=NZ-2 (h1) and K=NZ-3 (h2)
+                    // bottom wall: new values of planes K=NZ-2 and K=NZ-3, read back
+                    const double* ub = a.u_out + ucol;
+                    const size_t c1 = (size_t)(npz - 1) * a.uz, c2 = (size_t)(npz - 2) * a.uz;
+                    const double h1_ru = ub[F_RU * a.uf + c1], h1_rv = ub[F_RV * a.uf + c1];
+                    const double h1_ro = ub[F_RO * a.uf + c1], h1_tt = ub[F_TT * a.uf + c1];
+                    const double h2_ru = ub[F_RU * a.uf + c2], h2_rv = ub[F_RV * a.uf + c2];
+                    const double h2_ro = ub[F_RO * a.uf + c2], h2_tt = ub[F_TT * a.uf + c2];
                     const double ru_w = nr * (C43 * h1_ru / h1_ro - C13 * h2_ru / h2_ro);
                     const double rv_w = nr * (C43 * h1_rv / h1_ro - C13 * h2_rv / h2_ro);
                     const double tt_w = (s.izcon == 0) ? s.tb : C43 * h1_tt - C13 * h2_tt + s.bot_flux;
                     const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : nbz;
-                    uo[F_RU * a.fstride] = ru_w;
-                    uo[F_RV * a.fstride] = rv_w;
-                    uo[F_RW * a.fstride] = 0.0;
-                    uo[F_TT * a.fstride] = tt_w;
-                    if (MAG) uo[F_BZ * a.fstride] = bz_w;
+                    if (zok) {
+                        store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, kz, ru_w);
+                        store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, kz, rv_w);
+                        store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, kz, 0.0);
+                        store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, kz, tt_w);
+                        if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, kz, bz_w);
+                    }
                     if (STAGE == 3) {
                         CflPart cp;
                         cfl_cell<MAG>(s, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w, cell_dd(m, gi, gj, k), rka, cp);
@@ -555,22 +653,41 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const StageArgs a)
                         kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
                     }
                 }
-                h2_ru = h1_ru; h2_rv = h1_rv; h2_ro = h1_ro; h2_tt = h1_tt;
-                h1_ru = nu; h1_rv = nv; h1_ro = nr; h1_tt = nt;
             }
+        } else if (STAGE >= 2) {
+            // columns outside the domain still consume the Z fill of this plane
+            zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
+        }
+        if (!zok) atomicOr(sflag, 1);
+        if (STAGE >= 2) {
+            ++zfill;
+            if (tid == 0) zpending = false;
         }
         __syncthreads();
+        if (*sflag) break;
+        // refill: plane k+3 goes to the slot plane k-1 has left
+        if (tid == 0 && k + 3 <= k1) issue_plane(k + 3);
     }
-    if (STAGE == 3) {
-        __shared__ unsigned long long red[(NT / 32) * 6];
-        cfl_commit(a.acc, kw1, kw2, kw3, kw4, kmu, bad, red);
+    if (*sflag) {
+        // a bounded wait gave up: let every fill still in flight land (again
+        // bounded), report, and leave without touching the reduction
+        if (tid == 0) {
+            // the last fill of each slot is one of the four highest planes issued
+            for (int kp = hi_issued - 3; kp <= hi_issued; ++kp)
+                if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) & 3], parity_of(kp));
+            if (zpending) mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
+            atomicExch(&a.ctl->status, MHD3D_ERR_TIMEOUT);
+            atomicExch(&a.ctl->stop, 1);
+        }
+        return;
     }
+    if (STAGE == 3) cfl_commit(a.acc, kw1, kw2, kw3, kw4, kmu, bad, red);
 }
 
 // Standalone CFL reduction over the current state (STEP 3dmhdsub.f:741-873),
 // used before the first step and after a state change.
 template <bool MAG>
-__global__ void __launch_bounds__(NT) k_cfl(const StageArgs a)
+__global__ void __launch_bounds__(NT) k_cfl(const __grid_constant__ StageArgs a)
 {
     const Scalars& s = a.s;
     const int npx = s.npx, npy = s.npy, npz = s.npz;
@@ -581,12 +698,11 @@ __global__ void __launch_bounds__(NT) k_cfl(const StageArgs a)
         const int gi = (int)(q % npx);
         const int gj = (int)((q / npx) % npy);
         const int k = (int)(q / ((size_t)npx * npy));
-        const size_t c = (size_t)k * a.pstride + (size_t)gj * s.pitch + gi;
-        const double* u = a.u_in + c;
+        const double* u = a.u_in + (size_t)(k + 1) * a.uz + (size_t)(gj + 1) * a.upitch + (gi + 1);
         CflPart cp;
-        cfl_cell<MAG>(s, u[F_RU * a.fstride], u[F_RV * a.fstride], u[F_RW * a.fstride], u[F_RO * a.fstride],
-                      u[F_TT * a.fstride], MAG ? u[F_BX * a.fstride] : 0.0, MAG ? u[F_BY * a.fstride] : 0.0,
-                      MAG ? u[F_BZ * a.fstride] : 0.0, cell_dd(a.m, gi, gj, k), a.m.rkapa[k + 1], cp);
+        cfl_cell<MAG>(s, u[F_RU * a.uf], u[F_RV * a.uf], u[F_RW * a.uf], u[F_RO * a.uf], u[F_TT * a.uf],
+                      MAG ? u[F_BX * a.uf] : 0.0, MAG ? u[F_BY * a.uf] : 0.0, MAG ? u[F_BZ * a.uf] : 0.0,
+                      cell_dd(a.m, gi, gj, k), a.m.rkapa[k + 1], cp);
         kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
         kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
         kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
@@ -597,16 +713,17 @@ __global__ void __launch_bounds__(NT) k_cfl(const StageArgs a)
 
 // Standalone BCON on the current state, in place (test entry point).
 template <bool MAG>
-__global__ void __launch_bounds__(NT) k_bcon(const StageArgs a)
+__global__ void __launch_bounds__(NT) k_bcon(const __grid_constant__ StageArgs a)
 {
     const Scalars& s = a.s;
     const int npx = s.npx, npy = s.npy, npz = s.npz;
     const int q = blockIdx.x * NT + threadIdx.x;
     if (q >= npx * npy) return;
     const int gi = q % npx, gj = q / npx;
-    const size_t col = (size_t)gj * s.pitch + gi;
     double* u = const_cast<double*>(a.u_in);
-    auto at = [&](int f, int k) -> double& { return u[(size_t)f * a.fstride + (size_t)k * a.pstride + col]; };
+    const size_t col = (size_t)(gj + 1) * a.upitch + (gi + 1);
+    auto at = [&](int f, int k) -> double { return u[(size_t)f * a.uf + (size_t)(k + 1) * a.uz + col]; };
+    auto put = [&](int f, int k, double v) { store_u(u, (size_t)f * a.uf, a, gi, gj, k + 1, v); };
     const double C13 = s.c13, C23 = s.c23, C43 = s.c43;
     // top
     {
@@ -626,11 +743,11 @@ __global__ void __launch_bounds__(NT) k_bcon(const StageArgs a)
         } else if (s.itcon == 1) {
             tt_w = C43 * t1 - C13 * t2 - s.top_flux;
         }
-        at(F_RU, 0) = ru_w;
-        at(F_RV, 0) = rv_w;
-        at(F_RW, 0) = 0.0;
-        at(F_TT, 0) = tt_w;
-        if (MAG && s.ibcon == 0) at(F_BZ, 0) = 0.0;
+        put(F_RU, 0, ru_w);
+        put(F_RV, 0, rv_w);
+        put(F_RW, 0, 0.0);
+        put(F_TT, 0, tt_w);
+        if (MAG && s.ibcon == 0) put(F_BZ, 0, 0.0);
     }
     // bottom
     {
@@ -639,27 +756,32 @@ __global__ void __launch_bounds__(NT) k_bcon(const StageArgs a)
         const double ru_w = ro0 * (C43 * at(F_RU, kb - 1) / ro1 - C13 * at(F_RU, kb - 2) / ro2);
         const double rv_w = ro0 * (C43 * at(F_RV, kb - 1) / ro1 - C13 * at(F_RV, kb - 2) / ro2);
         const double tt_w = (s.izcon == 0) ? s.tb : C43 * at(F_TT, kb - 1) - C13 * at(F_TT, kb - 2) + s.bot_flux;
-        at(F_RU, kb) = ru_w;
-        at(F_RV, kb) = rv_w;
-        at(F_RW, kb) = 0.0;
-        at(F_TT, kb) = tt_w;
-        if (MAG && s.ibcon == 0) at(F_BZ, kb) = 0.0;
+        put(F_RU, kb, ru_w);
+        put(F_RV, kb, rv_w);
+        put(F_RW, kb, 0.0);
+        put(F_TT, kb, tt_w);
+        if (MAG && s.ibcon == 0) put(F_BZ, kb, 0.0);
     }
 }
 
 template <bool MAG, bool ROT>
 static cudaError_t launch_stage_t(int stage, const StageArgs& a, cudaStream_t st)
 {
-    constexpr int NQ = NQ_<MAG>::value;
-    const size_t smem = (size_t)3 * NQ * SX * SY * sizeof(double);
+    const size_t smem = Lay<MAG>::BYTES;
     const int nty = (a.s.npy + TY - 1) / TY;
     dim3 grid(a.ntx * nty, a.nchunks);
     switch (stage) {
-#define L_(S)                                                                                          \
-    case S: {                                                                                          \
-        cudaFuncSetAttribute(k_stage<MAG, ROT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        k_stage<MAG, ROT, S><<<grid, NT, smem, st>>>(a);                                              \
-        break;                                                                                         \
+#define L_(S)                                                                                              \
+    case S: {                                                                                              \
+        static bool attr_set = false;                                                                      \
+        if (!attr_set) {                                                                                   \
+            cudaError_t e = cudaFuncSetAttribute(k_stage<MAG, ROT, S>,                                     \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+            if (e != cudaSuccess) return e;                                                                \
+            attr_set = true;                                                                               \
+        }                                                                                                  \
+        k_stage<MAG, ROT, S><<<grid, NT, smem, st>>>(a);                                                  \
+        break;                                                                                             \
     }
         L_(0) L_(1) L_(2) L_(3)
 #undef L_
@@ -674,6 +796,8 @@ cudaError_t launch_stage(int stage, const StageArgs& a, cudaStream_t st)
     if (a.s.lmag) return a.s.lrot ? launch_stage_t<true, true>(stage, a, st) : launch_stage_t<true, false>(stage, a, st);
     return a.s.lrot ? launch_stage_t<false, true>(stage, a, st) : launch_stage_t<false, false>(stage, a, st);
 }
+
+size_t stage_smem_bytes(int lmag) { return lmag ? Lay<true>::BYTES : Lay<false>::BYTES; }
 
 cudaError_t launch_cfl(const StageArgs& a, cudaStream_t st)
 {
