@@ -16,13 +16,16 @@ struct CflPart {
     bool bad;
 };
 
+// The limits of one cell before the division of W2 by RKAPA(K):
+// X=0.5*DD*DD*REPR*CV*RO, so that W2=X/RKAPA(K) in the reference's order.
 template <bool MAG>
-__device__ __forceinline__ void cfl_cell(const Scalars& s, double ru, double rv, double rw, double ro, double tt,
-                                         double bx, double by, double bz, double dd, double rkapa, CflPart& c)
+__device__ __forceinline__ void cfl_terms(const Scalars& s, double ru, double rv, double rw, double ro, double tt,
+                                          double bx, double by, double bz, double dd, double& w1, double& x,
+                                          double& w3, double& mach2)
 {
     const double r = 1.0 / ro;
     const double uu = (ru * ru + rv * rv + rw * rw) * (r * r);
-    c.mach2 = s.ogamma * uu / tt;
+    mach2 = s.ogamma * uu / tt;
     double fast2;
     if (MAG) {
         const double b2o = (bx * bx + by * by + bz * bz) * s.obeta / ro;
@@ -30,9 +33,18 @@ __device__ __forceinline__ void cfl_cell(const Scalars& s, double ru, double rv,
     } else {
         fast2 = uu + s.gamma * tt + 2.0 * sqrt(uu * s.gamma * tt);
     }
-    c.w1 = dd / sqrt(fast2);
-    c.w2 = 0.5 * dd * dd * s.repr * s.cv * ro / rkapa;
-    c.w3 = 0.375 * dd * dd * s.re * ro;
+    w1 = dd / sqrt(fast2);
+    x = 0.5 * dd * dd * s.repr * s.cv * ro;
+    w3 = 0.375 * dd * dd * s.re * ro;
+}
+
+template <bool MAG>
+__device__ __forceinline__ void cfl_cell(const Scalars& s, double ru, double rv, double rw, double ro, double tt,
+                                         double bx, double by, double bz, double dd, double rkapa, CflPart& c)
+{
+    double x;
+    cfl_terms<MAG>(s, ru, rv, rw, ro, tt, bx, by, bz, dd, c.w1, x, c.w3, c.mach2);
+    c.w2 = x / rkapa;
     c.w4 = MAG ? 0.5 * dd * dd * s.rm : 0.0;
     c.bad = !(isfinite(c.w1) && isfinite(c.w2) && isfinite(c.w3) && isfinite(c.mach2));
 }

@@ -3,6 +3,7 @@
 // and the step loop with its device-side bookkeeping.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -37,7 +38,7 @@ struct Handle {
     Scalars s{};
     int ntx = 0, zlen = 0, nchunks = 0;
     bool dt_valid = false;
-    int gparity = 0;           // host copy of Control::gparity
+    unsigned long long w4key = ~0ull;   // key of min over cells of W4 (MHD), else ~0
     cudaStream_t own = nullptr;   // the handle's stream; st may be a caller's
     // asynchronous stepping: state at the last sync and steps enqueued since
     int nit_base = 0, cur_base = 0, pending = 0;
@@ -103,9 +104,10 @@ __global__ void k_pack_interior(const double* __restrict__ f, double* __restrict
     }
 }
 
-__global__ void k_reset(Control* ctl, Accum* acc, int clear_stop)
+__global__ void k_reset(Control* ctl, Accum* acc, int clear_stop, unsigned long long w4key)
 {
-    for (int i = 0; i < 4; ++i) acc->wmin[i] = ~0ull;
+    for (int i = 0; i < 3; ++i) acc->wmin[i] = ~0ull;
+    acc->wmin[3] = w4key;
     acc->umax = 0ull;
     acc->bad = 0u;
     if (clear_stop) {
@@ -117,7 +119,8 @@ __global__ void k_reset(Control* ctl, Accum* acc, int clear_stop)
 // End of a step (advance=1: NIT, TIMC, TIMT of STEP 3dmhdsub.f:1171-1173 and
 // the driver's DT check 3dmhd.f:924) and DT/UMACH of the next step from the
 // CFL accumulators (DT=SF*MIN(...), 3dmhdsub.f:866-873; UMACH=SQRT(...), 761).
-__global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance)
+__global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance,
+                           unsigned long long w4key)
 {
     if (advance) {
         if (ctl->stop) return;
@@ -126,7 +129,6 @@ __global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, in
         ctl->nit += 1;
         ctl->last_dt = ctl->dt;
         ctl->last_umach = ctl->umach;
-        ctl->gparity ^= 1;
         if (!(ctl->dt >= dtmin)) {
             ctl->stop = 1;
             ctl->status = isfinite(ctl->dt) ? MHD3D_ERR_DT_SMALL : MHD3D_ERR_NONFINITE;
@@ -143,7 +145,8 @@ __global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, in
         ctl->stop = 1;
         ctl->status = MHD3D_ERR_NONFINITE;
     }
-    for (int i = 0; i < 4; ++i) acc->wmin[i] = ~0ull;
+    for (int i = 0; i < 3; ++i) acc->wmin[i] = ~0ull;
+    acc->wmin[3] = w4key;
     acc->umax = 0ull;
     acc->bad = 0u;
 }
@@ -299,17 +302,20 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     CK(cudaMalloc(&h->ctl, sizeof(Control)));
     CK(cudaMalloc(&h->acc, sizeof(Accum)));
 
-    // 1-D arrays: 11 metric/kappa arrays and the two plume factors
-    const int lens[13] = {NX, NX, NX, NY, NY, NY, NZ, NZ, NZ, NZ, NZ, NX, NY};
+    // 1-D arrays: 11 metric/kappa arrays, the two plume factors, 9 fast-mode
+    // stencil factors, 4 fast-mode CFL factors
+    constexpr int NMET = 26;
+    const int lens[NMET] = {NX, NX, NX, NY, NY, NY, NZ, NZ, NZ, NZ, NZ, NX, NY,
+                            NX, NX, NX, NY, NY, NY, NZ, NZ, NZ, NX, NY, NZ, NZ};
     size_t tot = 0;
-    for (int i = 0; i < 13; ++i) tot += lens[i];
+    for (int i = 0; i < NMET; ++i) tot += lens[i];
     double* hm = (double*)std::malloc(sizeof(double) * tot);
     const double* exx = arrs[0];
     const double* wyy = arrs[4];
     const double* src[11] = {arrs[1], arrs[2], arrs[3], arrs[5], arrs[6], arrs[7], arrs[9], arrs[10], arrs[11],
                              arrs[12], arrs[13]};
     size_t off = 0;
-    size_t offs[13];
+    size_t offs[NMET];
     for (int i = 0; i < 11; ++i) {
         offs[i] = off;
         std::memcpy(hm + off, src[i], sizeof(double) * lens[i]);
@@ -331,6 +337,53 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
         hm[off + j] = plume ? std::exp(cln * (d * d)) : 0.0;
     }
     off += NY;
+    // fast-mode metric factors (products the reference forms per use)
+    {
+        const double* d1[3] = {src[0], src[3], src[6]};   // DXXDX, DYYDY, DZZDZ
+        const double* d2[3] = {src[1], src[4], src[7]};   // D2XXDX2, D2YYDY2, D2ZZDZ2
+        const double hh[3] = {p->hx, p->hy, p->hz}, h2[3] = {p->h2x, p->h2y, p->h2z};
+        const int len[3] = {NX, NY, NZ};
+        for (int d = 0; d < 3; ++d) {
+            offs[13 + 3 * d] = off;
+            for (int i = 0; i < len[d]; ++i) hm[off + i] = hh[d] * d1[d][i];
+            off += len[d];
+            offs[14 + 3 * d] = off;
+            for (int i = 0; i < len[d]; ++i) hm[off + i] = hh[d] * d2[d][i];
+            off += len[d];
+            offs[15 + 3 * d] = off;
+            for (int i = 0; i < len[d]; ++i) hm[off + i] = h2[d] * d1[d][i] * d1[d][i];
+            off += len[d];
+        }
+        // CFL: reciprocals of DDX, DDY, DDZ and W2's factor 0.5*REPR*CV/RKAPA(K)
+        const double* dd[3] = {src[2], src[5], src[8]};
+        for (int d = 0; d < 3; ++d) {
+            offs[22 + d] = off;
+            for (int i = 0; i < len[d]; ++i) hm[off + i] = 1.0 / dd[d][i];
+            off += len[d];
+        }
+        offs[25] = off;
+        for (int k = 0; k < NZ; ++k) hm[off + k] = 0.5 * p->repr * p->cv / src[9][k];
+        off += NZ;
+    }
+    // W4=0.5*DD*DD*RM (3dmhdsub.f:851) depends on the grid alone and is monotone
+    // in DD, so its minimum over the cells is that of the smallest or largest
+    // DD=MIN(DDX(I),DDY(J),DDZ(K)), I=2..NX-1, J=2..NY-1, K=2..NZ-1
+    if (p->lmag) {
+        double lo[3], hi[3];
+        const double* dd[3] = {src[2], src[5], src[8]};
+        const int n[3] = {npx, npy, npz};
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = hi[d] = dd[d][1];
+            for (int i = 2; i <= n[d]; ++i) {
+                lo[d] = dd[d][i] < lo[d] ? dd[d][i] : lo[d];
+                hi[d] = dd[d][i] > hi[d] ? dd[d][i] : hi[d];
+            }
+        }
+        const double dlo = std::min(std::min(lo[0], lo[1]), lo[2]);
+        const double dhi = std::min(std::min(hi[0], hi[1]), hi[2]);
+        const double f_lo = 0.5 * dlo * dlo * p->rm, f_hi = 0.5 * dhi * dhi * p->rm;
+        h->w4key = std::min(key_of(f_lo), key_of(f_hi));
+    }
     CK(cudaMalloc(&h->met, sizeof(double) * tot));
     CK(cudaMemcpy(h->met, hm, sizeof(double) * tot, cudaMemcpyHostToDevice));
     h->m.dxxdx = h->met + offs[0];
@@ -346,6 +399,19 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     h->m.dkapa = h->met + offs[10];
     h->m.plume_gx = h->met + offs[11];
     h->m.plume_gy = h->met + offs[12];
+    h->m.fax = h->met + offs[13];
+    h->m.fbx = h->met + offs[14];
+    h->m.fcx = h->met + offs[15];
+    h->m.fay = h->met + offs[16];
+    h->m.fby = h->met + offs[17];
+    h->m.fcy = h->met + offs[18];
+    h->m.faz = h->met + offs[19];
+    h->m.fbz = h->met + offs[20];
+    h->m.fcz = h->met + offs[21];
+    h->m.rddx = h->met + offs[22];
+    h->m.rddy = h->met + offs[23];
+    h->m.rddz = h->met + offs[24];
+    h->m.fw2z = h->met + offs[25];
 
     // scalars (3dmhd.f:105-240 values; FLUXES/BCON per-call products)
     Scalars& s = h->s;
@@ -360,6 +426,7 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     s.tmp_b = p->c43 * p->ocv * p->ore;
     s.tmp_13 = p->c13 * p->ore;
     s.tmp_m = p->obeta * p->orm * p->ocv;
+    s.cw3 = 0.375 * p->re;
     s.tb = p->tb; s.tp = p->tp; s.tc = p->tc; s.hh = p->hh;
     const double dzs = (double)(1.0f / (float)(npz - 1));
     s.top_dz = dzs / src[6][1];                         // DZ=1.0E00/FLOAT(NPZ-1)/DZZDZ(2)
@@ -375,7 +442,7 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
 
     // work decomposition: TX x TY tiles, z chunks of >= 3 planes
     h->ntx = (npx + TX - 1) / TX;
-    const int target = 64;
+    const int target = MHD3D_ZCHUNK;
     int nch = (npz + target - 1) / target;
     while (nch > 1 && npz / nch < 3) --nch;
     h->nchunks = nch;
@@ -386,7 +453,7 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     c0.timi = p->timi;
     c0.timt = 0.0;
     CK(cudaMemcpy(h->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice));
-    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1, h->w4key);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
     *out = h;
@@ -432,10 +499,10 @@ int download(Handle* h, double* const f[8])
 int initial_dt(Handle* h)
 {
     StageArgs a = make_args(h);
-    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+    k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1, h->w4key);
     CK(cudaGetLastError());
     CK(launch_cfl(h, a));
-    k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 0);
+    k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 0, h->w4key);
     CK(cudaGetLastError());
     h->dt_valid = true;
     return MHD3D_OK;
@@ -466,7 +533,7 @@ int step_async(Handle* h, int n)
         int st = initial_dt(h);
         if (st) return st;
     } else if (h->pending == 0) {
-        k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1);
+        k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1, h->w4key);
         CK(cudaGetLastError());
     }
     int cur = h->cur_base ^ (h->pending & 1);
@@ -487,7 +554,7 @@ int step_async(Handle* h, int n)
             }
             cur ^= 1;
         }
-        k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 1);
+        k_finalize<<<1, 1, 0, h->st>>>(h->ctl, h->acc, h->s.sf, h->s.dtmin, h->p.lmag, 1, h->w4key);
         CK(cudaGetLastError());
         h->pending += 1;
     }
@@ -507,7 +574,6 @@ int sync(Handle* h, double* dt, double* timc, double* timt, double* umach, int32
     h->cur_base = h->cur;
     h->nit_base = c.nit;
     h->pending = 0;
-    h->gparity = c.gparity;
     if (dt) *dt = c.last_dt;
     if (timc) *timc = c.timc;
     if (timt) *timt = c.timt;

@@ -20,8 +20,14 @@
 
 namespace mhd3d {
 
+#ifndef MHD3D_TY
+#define MHD3D_TY 4
+#endif
+#ifndef MHD3D_ZCHUNK
+#define MHD3D_ZCHUNK 64           // planes a CTA marches through (z chunk length target)
+#endif
 constexpr int TX = 32;            // tile width (one warp per row)
-constexpr int TY = 8;             // tile rows
+constexpr int TY = MHD3D_TY;      // tile rows (threads per CTA = 32*TY)
 constexpr int NT = TX * TY;       // threads per CTA
 constexpr int BW = TX + 2;        // TMA box row: x0-1 .. x0+TX
 constexpr int BH = TY + 2;        // TMA box rows: y0-1 .. y0+TY
@@ -43,6 +49,7 @@ struct Scalars {
     double tmp_b;      // C43*OCV*ORE       (1968, 2016)
     double tmp_13;     // C13*ORE           (1926, 2031, 2082)
     double tmp_m;      // OBETA*ORM*OCV     (2222, 2420, 2511)
+    double cw3;        // 0.375*RE, the factor of DD*DD*RO in W3 (fast-mode CFL)
     double tb, tp, tc, hh, theta_tp;
     double top_flux;   // C23*DZ*THETA at the top wall (ITC=1, 2856-2868)
     double top_dz;     // DZ at the top wall
@@ -61,7 +68,6 @@ struct Control {
     int nit;
     int stop;                     // nonzero: later stage kernels return at once
     int status;                   // MHD3D_* code behind stop
-    int gparity;                  // which gro copy is current at step start
 };
 
 // CFL accumulators: order-preserving 64-bit keys of doubles.
@@ -79,6 +85,10 @@ struct Metrics {
     const double *dzzdz, *d2zzdz2, *ddz;
     const double *rkapa, *dkapa;
     const double *plume_gx, *plume_gy;   // EXP(CLN*(EXX(I)-XP)**2), EXP(CLN*(WYY(J)-YP)**2)
+    // fast mode: HX*DXXDX, HX*D2XXDX2, H2X*DXXDX**2 and the same in y and z
+    const double *fax, *fbx, *fcx, *fay, *fby, *fcy, *faz, *fbz, *fcz;
+    // fast-mode CFL: 1/DDX, 1/DDY, 1/DDZ and 0.5*REPR*CV/RKAPA(K)
+    const double *rddx, *rddy, *rddz, *fw2z;
 };
 
 struct StageArgs {

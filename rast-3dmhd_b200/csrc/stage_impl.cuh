@@ -23,6 +23,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cfloat>
 
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
@@ -128,6 +129,179 @@ __device__ __forceinline__ void store_u(double* __restrict__ u, size_t fofs, con
     if (hx >= 0 && hy >= 0) u[base + (size_t)hy * a.upitch + hx] = v;
 }
 
+// ---- stage-3 CFL accumulation (STEP 3dmhdsub.f:741-873) ----
+// DT=SF*MIN(W1,W2,W3,W4) needs only the minimum over all cells of the four
+// limits together, and UMACH the maximum of MACH**2.  W4=0.5*DD*DD*RM depends
+// on the grid alone: the host folds its minimum into the accumulator's start
+// value.  Each warp keeps one slot of three words in shared memory: the
+// limits' minimum key, MACH**2's maximum key and the non-finite flag.
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+#if MHD3D_FAST_BODY
+// Contracted form: W1=DD/(|u|+c_f) (SQRT(FAST2) of the reference is |u|+c_f
+// exactly, c_f**2=GAMMA*TT+B**2*OBETA/RO), reduced as max((|u|+c_f)/DD);
+// W3 and W2 are 0.375*RE*Y and (0.5*REPR*CV/RKAPA(K))*Y with Y=DD*DD*RO; one
+// reciprocal of RO*TT serves 1/RO and 1/TT.
+struct CflAcc {
+    double smax = 0.0;        // max over cells of (|u|+c_f)/DD
+    double wmin = __builtin_huge_val();   // min of W2, W3
+    double m2 = -__builtin_huge_val();    // max of MACH**2
+    unsigned bad = 0;
+};
+
+template <bool MAG>
+__device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const Metrics& m, int gi, int gj, int kd,
+                                             double ru, double rv, double rw, double ro, double tt, double bx,
+                                             double by, double bz)
+{
+    const double rp = 1.0 / (ro * tt);
+    const double r = tt * rp;
+    const double uu = (ru * ru + rv * rv + rw * rw) * (r * r);
+    const double mach2 = s.ogamma * uu * (ro * rp);
+    double a2 = s.gamma * tt;
+    if (MAG) a2 += (bx * bx + by * by + bz * bz) * s.obeta * r;
+    const double sp = (uu > 0.0 ? uu * rsqrt(uu) : 0.0) + a2 * rsqrt(a2);
+    const double rdd = fmax(fmax(m.rddx[gi + 1], m.rddy[gj + 1]), m.rddz[kd + 1]);
+    const double dd = dmin(dmin(m.ddx[gi + 1], m.ddy[gj + 1]), m.ddz[kd + 1]);
+    const double sr = sp * rdd;
+    const double y = dd * dd * ro;
+    const double w = fmin(s.cw3 * y, m.fw2z[kd + 1] * y);
+    c.smax = fmax(c.smax, sr);
+    c.wmin = fmin(c.wmin, w);
+    c.m2 = fmax(c.m2, mach2);
+    c.bad |= (unsigned)(!(sr > 0.0 && sr <= DBL_MAX) || !(fabs(w) <= DBL_MAX) || !(fabs(mach2) <= DBL_MAX));
+}
+
+// the top wall's cells (formed in the pass of plane 3): nothing plane-bound
+template <bool MAG>
+__device__ __forceinline__ void cfl_acc_direct(CflAcc& c, const Scalars& s, const Metrics& m, int gi, int gj, int kd,
+                                               double ru, double rv, double rw, double ro, double tt, double bx,
+                                               double by, double bz)
+{
+    cfl_acc_cell<MAG>(c, s, m, gi, gj, kd, ru, rv, rw, ro, tt, bx, by, bz);
+}
+
+__device__ __forceinline__ void cfl_fold_plane(unsigned long long*, CflAcc&, double) {}
+
+__device__ __forceinline__ void cfl_commit_acc(Accum* acc, unsigned long long* red, CflAcc& c)
+{
+    double smax = c.smax, wmin = c.wmin, m2 = c.m2;
+    unsigned bad = c.bad;
+    for (int o = 16; o > 0; o >>= 1) {
+        smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        wmin = fmin(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+        m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    unsigned long long* r = red + (threadIdx.x >> 5) * 3;
+    if ((threadIdx.x & 31) == 0) {
+        if (smax > 0.0) wmin = fmin(wmin, 1.0 / smax);
+        r[0] = min(r[0], key_of(wmin));
+        r[1] = max(r[1], key_of(m2));
+        r[2] |= bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long kmin = ~0ull, kmu = 0ull, b = 0ull;
+        for (int i = 0; i < NT / 32; ++i) {
+            kmin = min(kmin, red[i * 3 + 0]);
+            kmu = max(kmu, red[i * 3 + 1]);
+            b |= red[i * 3 + 2];
+        }
+        atomicMin(&acc->wmin[0], kmin);
+        atomicMax(&acc->umax, kmu);
+        if (b) atomicOr(&acc->bad, 1u);
+    }
+}
+#else
+// Reference rounding: every limit as STEP forms it.  W2=X/RKAPA(K) with
+// X=0.5*DD*DD*REPR*CV*RO is reduced per plane: RKAPA(K) is one value over a
+// plane and X->X/RKAPA(K) is monotone (correctly rounded), so the plane's
+// minimum of W2 is min(Xmin/RKAPA(K), Xmax/RKAPA(K)) bit for bit, and W2 is
+// non-finite somewhere on the plane exactly when X is or one of those two is.
+struct CflAcc {
+    unsigned long long kmin = ~0ull, kmu = 0ull;    // W1, W3 (and direct W2); MACH**2
+    unsigned long long kxmin = ~0ull, kxmax = 0ull; // X over this plane
+    unsigned bad = 0;
+};
+
+template <bool MAG>
+__device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const Metrics& m, int gi, int gj, int kd,
+                                             double ru, double rv, double rw, double ro, double tt, double bx,
+                                             double by, double bz)
+{
+    double w1, x, w3, mach2;
+    cfl_terms<MAG>(s, ru, rv, rw, ro, tt, bx, by, bz, cell_dd(m, gi, gj, kd), w1, x, w3, mach2);
+    c.kmin = min(c.kmin, min(key_of(w1), key_of(w3)));
+    c.kxmin = min(c.kxmin, key_of(x));
+    c.kxmax = max(c.kxmax, key_of(x));
+    c.kmu = max(c.kmu, key_of(mach2));
+    c.bad |= (unsigned)!(isfinite(w1) && isfinite(x) && isfinite(w3) && isfinite(mach2));
+}
+
+// a cell whose RKAPA is not that of the plane being folded (the top wall's,
+// formed in the pass of plane 3)
+template <bool MAG>
+__device__ __forceinline__ void cfl_acc_direct(CflAcc& c, const Scalars& s, const Metrics& m, int gi, int gj, int kd,
+                                               double ru, double rv, double rw, double ro, double tt, double bx,
+                                               double by, double bz)
+{
+    CflPart cp;
+    cfl_cell<MAG>(s, ru, rv, rw, ro, tt, bx, by, bz, cell_dd(m, gi, gj, kd), m.rkapa[kd + 1], cp);
+    c.kmin = min(c.kmin, min(min(key_of(cp.w1), key_of(cp.w2)), key_of(cp.w3)));
+    c.kmu = max(c.kmu, key_of(cp.mach2));
+    c.bad |= (unsigned)cp.bad;
+}
+
+// end of a plane: W2 of the plane's cells from the warp's X range
+__device__ __forceinline__ void cfl_fold_plane(unsigned long long* red, CflAcc& c, double rk)
+{
+    const unsigned long long xlo = warp_min_u64(c.kxmin), xhi = warp_max_u64(c.kxmax);
+    c.kxmin = ~0ull;
+    c.kxmax = 0ull;
+    if ((threadIdx.x & 31) == 0 && xlo != ~0ull) {
+        const double a = of_key(xlo) / rk, b = of_key(xhi) / rk;
+        unsigned long long* r = red + (threadIdx.x >> 5) * 3;
+        r[0] = min(r[0], min(key_of(a), key_of(b)));
+        if (!(isfinite(a) && isfinite(b))) r[2] = 1ull;
+    }
+}
+
+__device__ __forceinline__ void cfl_commit_acc(Accum* acc, unsigned long long* red, CflAcc& c)
+{
+    const unsigned long long kmin = warp_min_u64(c.kmin), kmu = warp_max_u64(c.kmu);
+    unsigned bad = c.bad;
+    for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    unsigned long long* r = red + (threadIdx.x >> 5) * 3;
+    if ((threadIdx.x & 31) == 0) {
+        r[0] = min(r[0], kmin);
+        r[1] = max(r[1], kmu);
+        r[2] |= bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long k1 = ~0ull, km = 0ull, b = 0ull;
+        for (int i = 0; i < NT / 32; ++i) {
+            k1 = min(k1, red[i * 3 + 0]);
+            km = max(km, red[i * 3 + 1]);
+            b |= red[i * 3 + 2];
+        }
+        atomicMin(&acc->wmin[0], k1);
+        atomicMax(&acc->umax, km);
+        if (b) atomicOr(&acc->bad, 1u);
+    }
+}
+#endif
+
 // Block-wide reduction of the CFL parts into the global accumulators.
 __device__ __forceinline__ void cfl_commit(Accum* acc, unsigned long long k1, unsigned long long k2,
                                            unsigned long long k3, unsigned long long k4, unsigned long long km,
@@ -175,7 +349,10 @@ __device__ __forceinline__ void cfl_commit(Accum* acc, unsigned long long k1, un
 // STAGE 1..3: the RK3 substeps of STEP (3dmhdsub.f:874-1169).
 // ---------------------------------------------------------------------------
 template <bool MAG, bool ROT, int STAGE>
-__global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageArgs a)
+#ifndef MHD3D_MINB
+#define MHD3D_MINB 3   // CTAs per SM: 3 x 128 threads x 168 registers, 3 x 65 KB shared
+#endif
+__global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant__ StageArgs a)
 {
     using L = Lay<MAG>;
     constexpr int NF = L::NF;
@@ -213,9 +390,12 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
     const double dyj = active ? m.dyydy[gj + 1] : 0.0, d2yj = active ? m.d2yydy2[gj + 1] : 0.0;
     const double HX = s.hx, H2X = s.h2x, HY = s.hy, H2Y = s.h2y, HZ = s.hz, H2Z = s.h2z;
     const double C13 = s.c13, C23 = s.c23, C43 = s.c43, OCV = s.ocv, ORE = s.ore;
-
-    unsigned long long kw1 = ~0ull, kw2 = ~0ull, kw3 = ~0ull, kw4 = ~0ull, kmu = 0ull;
-    unsigned int bad = 0;
+#if MHD3D_FAST_BODY
+    // d/dx ~ (f+ - f-)*ax, d2/dx2 ~ (f+ - f-)*bxq + (f+ + f- - 2f)*cxq, likewise in y and z
+    const double ax = active ? m.fax[gi + 1] : 0.0, bxq = active ? m.fbx[gi + 1] : 0.0, cxq = active ? m.fcx[gi + 1] : 0.0;
+    const double ay = active ? m.fay[gj + 1] : 0.0, byq = active ? m.fby[gj + 1] : 0.0, cyq = active ? m.fcy[gj + 1] : 0.0;
+    (void)HX; (void)H2X; (void)HY; (void)H2Y; (void)HZ; (void)H2Z; (void)OCV; (void)ORE; (void)dxi; (void)d2xi; (void)dyj; (void)d2yj;
+#endif
 
     const unsigned raw_bytes = (unsigned)(NF * BSLOT * 8);
     const unsigned z_bytes = (unsigned)(NF * TY * TX * 8);
@@ -228,6 +408,12 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
         for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
         *sflag = 0;
         fence_mbar_init();
+    }
+    if (STAGE == 3 && (tid & 31) == 0) {
+        unsigned long long* r = red + (tid >> 5) * 3;
+        r[0] = ~0ull;
+        r[1] = 0ull;
+        r[2] = 0ull;
     }
     __syncthreads();
 
@@ -259,6 +445,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
     }
     bool zpending = false;   // thread 0: a Z fill is in flight
     int zfill = 0;           // fills of the Z barrier so far
+    CflAcc cfa;              // stage-3 CFL parts of this thread's cells
 
     for (int k = k0; k < k1; ++k) {
         if (STAGE >= 2 && tid == 0 && !*sflag) {
@@ -298,6 +485,142 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
             by3 = a.u_in[c3 + F_BY * a.uf];                                                          \
         }                                                                                            \
     }
+#if MHD3D_FAST_BODY
+            const bool top = (k == 0), bot = (k == npz - 1);
+            const double az = m.faz[k + 1], bzq = m.fbz[k + 1], czq = m.fcz[k + 1];
+            const double rka = m.rkapa[k + 1], dka = m.dkapa[k + 1];
+            WALL_LOADS
+
+            // center
+            const double RIc = C_(Q_RI, 0, 0), ROc = C_(Q_RO, 0, 0), TTc = C_(Q_TT, 0, 0);
+            const double RUc = C_(Q_RU, 0, 0), RVc = C_(Q_RV, 0, 0), RWc = C_(Q_RW, 0, 0);
+            const double BXc0 = MAG ? C_(Q_BX, 0, 0) : 0.0, BYc0 = MAG ? C_(Q_BY, 0, 0) : 0.0;
+            const double BZc0 = MAG ? C_(Q_BZ, 0, 0) : 0.0;
+            const double uc = RUc * RIc, vc = RVc * RIc, wc = RWc * RIc;
+            // face neighbours: velocities (the products FLUXES forms) and momenta
+            const double u_xp = C_(Q_UU, 1, 0), u_xm = C_(Q_UU, -1, 0), u_yp = C_(Q_UU, 0, 1), u_ym = C_(Q_UU, 0, -1);
+            const double v_xp = C_(Q_VV, 1, 0), v_xm = C_(Q_VV, -1, 0), v_yp = C_(Q_VV, 0, 1), v_ym = C_(Q_VV, 0, -1);
+            const double w_xp = C_(Q_WW, 1, 0), w_xm = C_(Q_WW, -1, 0), w_yp = C_(Q_WW, 0, 1), w_ym = C_(Q_WW, 0, -1);
+            const double u_zp = P_(Q_UU, 0, 0), u_zm = M_(Q_UU, 0, 0);
+            const double v_zp = P_(Q_VV, 0, 0), v_zm = M_(Q_VV, 0, 0);
+            const double w_zp = P_(Q_WW, 0, 0), w_zm = M_(Q_WW, 0, 0);
+
+            // ---- continuity (3dmhdsub.f:1258-1295), one-sided d(RW)/dz on the walls
+            double dzrw;
+            if (top) dzrw = (4.0 * P_(Q_RW, 0, 0) - rw2) * az;
+            else if (bot) dzrw = (rw2 - 4.0 * M_(Q_RW, 0, 0)) * az;
+            else dzrw = (P_(Q_RW, 0, 0) - M_(Q_RW, 0, 0)) * az;
+            double fr = -((C_(Q_RU, 1, 0) - C_(Q_RU, -1, 0)) * ax + (C_(Q_RV, 0, 1) - C_(Q_RV, 0, -1)) * ay) - dzrw;
+            // ---- buoyancy, pressure gradient, advection (1376-1482)
+            double fu = -((C_(Q_P, 1, 0) - C_(Q_P, -1, 0)) * ax
+                          + (C_(Q_RU, 1, 0) * u_xp - C_(Q_RU, -1, 0) * u_xm) * ax
+                          + (C_(Q_RU, 0, 1) * v_yp - C_(Q_RU, 0, -1) * v_ym) * ay
+                          + (P_(Q_RU, 0, 0) * w_zp - M_(Q_RU, 0, 0) * w_zm) * az);
+            double fv = -((C_(Q_P, 0, 1) - C_(Q_P, 0, -1)) * ay
+                          + (C_(Q_RV, 1, 0) * u_xp - C_(Q_RV, -1, 0) * u_xm) * ax
+                          + (C_(Q_RV, 0, 1) * v_yp - C_(Q_RV, 0, -1) * v_ym) * ay
+                          + (P_(Q_RV, 0, 0) * w_zp - M_(Q_RV, 0, 0) * w_zm) * az);
+            double fw = s.grav * ROc
+                      - ((P_(Q_P, 0, 0) - M_(Q_P, 0, 0)) * az
+                         + (C_(Q_RW, 1, 0) * u_xp - C_(Q_RW, -1, 0) * u_xm) * ax
+                         + (C_(Q_RW, 0, 1) * v_yp - C_(Q_RW, 0, -1) * v_ym) * ay
+                         + (P_(Q_RW, 0, 0) * w_zp - M_(Q_RW, 0, 0) * w_zm) * az);
+            // ---- temperature advection and conduction (1495-1506, 1583-1611)
+            double ft;
+            {
+                const double txp = C_(Q_TT, 1, 0), txm = C_(Q_TT, -1, 0);
+                const double typ = C_(Q_TT, 0, 1), tym = C_(Q_TT, 0, -1);
+                const double tzp = P_(Q_TT, 0, 0), tzm = M_(Q_TT, 0, 0);
+                const double dtx = txp - txm, dty = typ - tym, dtz = tzp - tzm;
+                const double lap = dtx * bxq + (txp + txm - 2.0 * TTc) * cxq + dty * byq + (typ + tym - 2.0 * TTc) * cyq
+                                 + dtz * bzq + (tzp + tzm - 2.0 * TTc) * czq;
+                ft = -(uc * dtx * ax + vc * dty * ay + wc * dtz * az) + RIc * s.tmp_cond * (rka * lap + dka * dtz * az);
+            }
+            // ---- viscous stress (1818-1886)
+            {
+                const double lxu = (u_xp - u_xm) * bxq + (u_xp + u_xm - 2.0 * uc) * cxq;
+                const double lyu = (u_yp - u_ym) * byq + (u_yp + u_ym - 2.0 * uc) * cyq;
+                const double lzu = (u_zp - u_zm) * bzq + (u_zp + u_zm - 2.0 * uc) * czq;
+                const double lxv = (v_xp - v_xm) * bxq + (v_xp + v_xm - 2.0 * vc) * cxq;
+                const double lyv = (v_yp - v_ym) * byq + (v_yp + v_ym - 2.0 * vc) * cyq;
+                const double lzv = (v_zp - v_zm) * bzq + (v_zp + v_zm - 2.0 * vc) * czq;
+                const double lxw = (w_xp - w_xm) * bxq + (w_xp + w_xm - 2.0 * wc) * cxq;
+                const double lyw = (w_yp - w_ym) * byq + (w_yp + w_ym - 2.0 * wc) * cyq;
+                const double lzw = (w_zp - w_zm) * bzq + (w_zp + w_zm - 2.0 * wc) * czq;
+                fu += s.ore * (s.c43 * lxu + lyu + lzu);
+                fv += s.ore * (lxv + s.c43 * lyv + lzv);
+                fw += s.ore * (lxw + lyw + s.c43 * lzw);
+            }
+            // ---- velocity gradients, the 19-point cross terms, heating (1891-2101)
+            const double ux = (u_xp - u_xm) * ax, vx = (v_xp - v_xm) * ax, wx = (w_xp - w_xm) * ax;
+            const double uy = (u_yp - u_ym) * ay, vy = (v_yp - v_ym) * ay, wy = (w_yp - w_ym) * ay;
+            const double uz = (u_zp - u_zm) * az, vz = (v_zp - v_zm) * az, wz = (w_zp - w_zm) * az;
+            {
+                const double axy = ax * ay, axz = ax * az, ayz = ay * az;
+                const double dyvx = ((C_(Q_VV, 1, 1) - C_(Q_VV, -1, 1)) - (C_(Q_VV, 1, -1) - C_(Q_VV, -1, -1))) * axy;
+                const double dyux = ((C_(Q_UU, 1, 1) - C_(Q_UU, -1, 1)) - (C_(Q_UU, 1, -1) - C_(Q_UU, -1, -1))) * axy;
+                const double dxwz = ((P_(Q_WW, 1, 0) - M_(Q_WW, 1, 0)) - (P_(Q_WW, -1, 0) - M_(Q_WW, -1, 0))) * axz;
+                const double dywz = ((P_(Q_WW, 0, 1) - M_(Q_WW, 0, 1)) - (P_(Q_WW, 0, -1) - M_(Q_WW, 0, -1))) * ayz;
+                const double dxuz = ((P_(Q_UU, 1, 0) - M_(Q_UU, 1, 0)) - (P_(Q_UU, -1, 0) - M_(Q_UU, -1, 0))) * axz;
+                const double dyvz = ((P_(Q_VV, 0, 1) - M_(Q_VV, 0, 1)) - (P_(Q_VV, 0, -1) - M_(Q_VV, 0, -1))) * ayz;
+                fu += s.tmp_13 * (dyvx + dxwz);
+                fv += s.tmp_13 * (dyux + dywz);
+                fw += s.tmp_13 * (dxuz + dyvz);
+            }
+            double heat = s.tmp_a * (s.c43 * ux * ux + vx * vx + wx * wx + uy * uy + 2.0 * uy * vx + uz * uz + vz * vz
+                                     + wy * wy + 2.0 * vz * wy + 2.0 * uz * wx)
+                        + s.tmp_b * (vy * vy + wz * wz - ux * wz - ux * vy - vy * wz);
+            ft -= s.ocv * TTc * (ux + vy + wz);
+            // ---- Coriolis (2106-2125)
+            if (ROT) {
+                fu += s.omz * RVc;
+                fv += s.omx * RWc - s.omz * RUc;
+                fw -= s.omx * RVc;
+            }
+            // ---- induction, Lorentz force, Ohmic heating (2129-2634)
+            double w1 = 0, w2 = 0, w3 = 0;
+            if (MAG) {
+                const double BXc = BXc0, BYc = BYc0, BZc = BZc0;
+                const double bxxp = C_(Q_BX, 1, 0), bxxm = C_(Q_BX, -1, 0), bxyp = C_(Q_BX, 0, 1), bxym = C_(Q_BX, 0, -1);
+                const double byxp = C_(Q_BY, 1, 0), byxm = C_(Q_BY, -1, 0), byyp = C_(Q_BY, 0, 1), byym = C_(Q_BY, 0, -1);
+                const double bzxp = C_(Q_BZ, 1, 0), bzxm = C_(Q_BZ, -1, 0), bzyp = C_(Q_BZ, 0, 1), bzym = C_(Q_BZ, 0, -1);
+                const double bxzp = P_(Q_BX, 0, 0), bxzm = M_(Q_BX, 0, 0);
+                const double byzp = P_(Q_BY, 0, 0), byzm = M_(Q_BY, 0, 0);
+                const double bzzp = P_(Q_BZ, 0, 0), bzzm = M_(Q_BZ, 0, 0);
+                const double bxx = (bxxp - bxxm) * ax, byx = (byxp - byxm) * ax, bzx = (bzxp - bzxm) * ax;
+                const double bxy = (bxyp - bxym) * ay, byy = (byyp - byym) * ay, bzy = (bzyp - bzym) * ay;
+                const double bxz = (bxzp - bxzm) * az, byz = (byzp - byzm) * az, bzz = (bzzp - bzzm) * az;
+                double wzm = wz, lzbx, lzby;
+                if (top) {
+                    wzm = (4.0 * w_zp - ww2) * az;
+                    lzbx = (-3.0 * BXc + 4.0 * bxzp - bx2) * bzq + (2.0 * BXc - 5.0 * bxzp + 4.0 * bx2 - bx3) * czq;
+                    lzby = (-3.0 * BYc + 4.0 * byzp - by2) * bzq + (2.0 * BYc - 5.0 * byzp + 4.0 * by2 - by3) * czq;
+                } else if (bot) {
+                    wzm = (ww2 - 4.0 * w_zm) * az;
+                    lzbx = (3.0 * BXc - 4.0 * bxzm + bx2) * bzq + (2.0 * BXc - 5.0 * bxzm + 4.0 * bx2 - bx3) * czq;
+                    lzby = (3.0 * BYc - 4.0 * byzm + by2) * bzq + (2.0 * BYc - 5.0 * byzm + 4.0 * by2 - by3) * czq;
+                } else {
+                    lzbx = (bxzp - bxzm) * bzq + (bxzp + bxzm - 2.0 * BXc) * czq;
+                    lzby = (byzp - byzm) * bzq + (byzp + byzm - 2.0 * BYc) * czq;
+                }
+                const double lbx = (bxxp - bxxm) * bxq + (bxxp + bxxm - 2.0 * BXc) * cxq
+                                 + (bxyp - bxym) * byq + (bxyp + bxym - 2.0 * BXc) * cyq + lzbx;
+                const double lby = (byxp - byxm) * bxq + (byxp + byxm - 2.0 * BYc) * cxq
+                                 + (byyp - byym) * byq + (byyp + byym - 2.0 * BYc) * cyq + lzby;
+                const double lbz = (bzxp - bzxm) * bxq + (bzxp + bzxm - 2.0 * BZc) * cxq
+                                 + (bzyp - bzym) * byq + (bzyp + bzym - 2.0 * BZc) * cyq
+                                 + (bzzp - bzzm) * bzq + (bzzp + bzzm - 2.0 * BZc) * czq;
+                w1 = BYc * uy - BXc * vy + BZc * uz - BXc * wzm - (uc * bxx + vc * bxy + wc * bxz) + s.orm * lbx;
+                w2 = BXc * vx - BYc * ux + BZc * vz - BYc * wzm - (uc * byx + vc * byy + wc * byz) + s.orm * lby;
+                w3 = BXc * wx - BZc * ux + BYc * wy - BZc * vy - (uc * bzx + vc * bzy + wc * bzz) + s.orm * lbz;
+                const double jz = bxy - byx, jy = bxz - bzx, jx = byz - bzy;
+                fu += s.obeta * (BYc * jz + BZc * jy);
+                fv += s.obeta * (BZc * jx - BXc * jz);
+                fw -= s.obeta * (BXc * jy + BYc * jx);
+                heat += s.tmp_m * (jx * jx + jy * jy + jz * jz);
+            }
+            ft += RIc * heat;
+#else
             const bool top = (k == 0), bot = (k == npz - 1);
             const double dzk = m.dzzdz[k + 1], d2zk = m.d2zzdz2[k + 1];
             const double rka = m.rkapa[k + 1], dka = m.dkapa[k + 1];
@@ -497,6 +820,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
                 const double bzz2 = (bzzp - bzzm) * HZ * d2zk + (bzzp - 2.0 * BZc + bzzm) * H2Z * dzk * dzk;  // 1570
                 w3 = w3 + ORM * bzz2;                                            // 1580
             }
+#endif
             // ghost RO planes: this FLUXES call leaves 1/RO behind (3dmhdsub.f:1386-1391)
             if (STAGE != 0) {
                 if (top) store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, 0, M_(Q_RI, 0, 0));
@@ -577,13 +901,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
                 }
                 // ---- BCON (3dmhdsub.f:2751-2955) and the CFL parts of the next step
                 if (!top && !bot) {
-                    if (STAGE == 3) {
-                        CflPart cp;
-                        cfl_cell<MAG>(s, nu, nv, nw, nr, nt, nbx, nby, nbz, cell_dd(m, gi, gj, k), rka, cp);
-                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
-                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
-                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
-                    }
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, nu, nv, nw, nr, nt, nbx, nby, nbz);
                 }
                 if (k == 2 && k0 == 0) {
                     // top wall: new values of planes K=3 (read back) and K=4 (this plane);
@@ -617,14 +935,8 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
                         store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, 1, tt_w);
                         if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, 1, bz_w);
                     }
-                    if (STAGE == 3) {
-                        CflPart cp;
-                        cfl_cell<MAG>(s, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w, cell_dd(m, gi, gj, 0),
-                                      m.rkapa[1], cp);
-                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
-                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
-                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
-                    }
+                    if (STAGE == 3)
+                        cfl_acc_direct<MAG>(cfa, s, m, gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
                 }
                 if (bot) {
                     // bottom wall: new values of planes K=NZ-2 and K=NZ-3, read back
@@ -645,13 +957,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
                         store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, kz, tt_w);
                         if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, kz, bz_w);
                     }
-                    if (STAGE == 3) {
-                        CflPart cp;
-                        cfl_cell<MAG>(s, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w, cell_dd(m, gi, gj, k), rka, cp);
-                        kw1 = min(kw1, key_of(cp.w1)); kw2 = min(kw2, key_of(cp.w2));
-                        kw3 = min(kw3, key_of(cp.w3)); kw4 = min(kw4, key_of(cp.w4));
-                        kmu = max(kmu, key_of(cp.mach2)); bad |= cp.bad;
-                    }
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
                 }
             }
         } else if (STAGE >= 2) {
@@ -659,6 +965,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
             zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
         }
         if (!zok) atomicOr(sflag, 1);
+        if (STAGE == 3) cfl_fold_plane(red, cfa, m.rkapa[k + 1]);
         if (STAGE >= 2) {
             ++zfill;
             if (tid == 0) zpending = false;
@@ -681,7 +988,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(const __grid_constant__ StageAr
         }
         return;
     }
-    if (STAGE == 3) cfl_commit(a.acc, kw1, kw2, kw3, kw4, kmu, bad, red);
+    if (STAGE == 3) cfl_commit_acc(a.acc, red, cfa);
 }
 
 // Standalone CFL reduction over the current state (STEP 3dmhdsub.f:741-873),
