@@ -129,6 +129,45 @@ __device__ __forceinline__ void store_u(double* __restrict__ u, size_t fofs, con
     if (hx >= 0 && hy >= 0) u[base + (size_t)hy * a.upitch + hx] = v;
 }
 
+// Periodic halo copies of one interior column: plane offsets of the copies
+// COMMUNICATE makes at I=1/NX and J=1/NY, formed once per thread.
+struct HaloCols {
+    int hx, hy, hxy;   // x copy, y copy, corner copy
+    bool ex, ey;
+};
+__device__ __forceinline__ HaloCols halo_cols(const StageArgs& a, int gi, int gj)
+{
+    const int npx = a.s.npx, npy = a.s.npy;
+    const int cx = (gi == 0) ? npx + 1 : (gi == npx - 1) ? 0 : -1;
+    const int cy = (gj == 0) ? npy + 1 : (gj == npy - 1) ? 0 : -1;
+    HaloCols h;
+    h.ex = cx >= 0;
+    h.ey = cy >= 0;
+    h.hx = (gj + 1) * a.upitch + cx;
+    h.hy = cy * a.upitch + (gi + 1);
+    h.hxy = cy * a.upitch + cx;
+    return h;
+}
+
+// store N fields of one cell of U (pl: the plane's base) and their halo
+// copies; the copies are one branch for the columns that have none
+template <int N>
+__device__ __forceinline__ void store_cell(double* __restrict__ pl, size_t uf, size_t ucol, const HaloCols& h,
+                                           const int (&f)[N], const double (&v)[N])
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i) pl[(size_t)f[i] * uf + ucol] = v[i];
+    if (h.ex || h.ey) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double* q = pl + (size_t)f[i] * uf;
+            if (h.ex) q[h.hx] = v[i];
+            if (h.ey) q[h.hy] = v[i];
+            if (h.ex && h.ey) q[h.hxy] = v[i];
+        }
+    }
+}
+
 // ---- stage-3 CFL accumulation (STEP 3dmhdsub.f:741-873) ----
 // DT=SF*MIN(W1,W2,W3,W4) needs only the minimum over all cells of the four
 // limits together, and UMACH the maximum of MACH**2.  W4=0.5*DD*DD*RM depends
@@ -356,8 +395,10 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
 {
     using L = Lay<MAG>;
     constexpr int NF = L::NF;
-    extern __shared__ unsigned char smem_raw[];
-    double* const sbase = reinterpret_cast<double*>((reinterpret_cast<size_t>(smem_raw) + 127) & ~(size_t)127);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned base, formed by pointer arithmetic on the shared array
+    // so that every access below stays a shared-window (32-bit) access
+    double* const sbase = reinterpret_cast<double*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
     double* const sraw = sbase;
     double* const sri = sbase + L::RI_OFF;
     double* const sz = sbase + L::Z_OFF;
@@ -403,6 +444,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     // ghost planes at 0 and NPZ+1) and in the compact Z/F layout
     const size_t ucol = (size_t)(gj + 1) * a.upitch + (gi + 1);
     const size_t zcol = (size_t)gj * a.zpitch + gi;
+    const HaloCols hc = halo_cols(a, gi, gj);
 
     if (tid == 0) {
         for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
@@ -823,8 +865,8 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
 #endif
             // ghost RO planes: this FLUXES call leaves 1/RO behind (3dmhdsub.f:1386-1391)
             if (STAGE != 0) {
-                if (top) store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, 0, M_(Q_RI, 0, 0));
-                if (bot) store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, npz + 1, P_(Q_RI, 0, 0));
+                if (top) store_cell<1>(a.u_out, a.uf, ucol, hc, {F_RO}, {M_(Q_RI, 0, 0)});
+                if (bot) store_cell<1>(a.u_out + (size_t)(npz + 1) * a.uz, a.uf, ucol, hc, {F_RO}, {P_(Q_RI, 0, 0)});
             }
 #undef C_
 #undef M_
@@ -870,17 +912,13 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                 const double nbx = zbx + cu * w1, nby = zby + cu * w2, nbz = zbz + cu * w3;
                 const int kz = k + 1;
                 if (zok) {
-                    store_u(a.u_out, (size_t)F_RO * a.uf, a, gi, gj, kz, nr);
-                    if (MAG) {
-                        store_u(a.u_out, (size_t)F_BX * a.uf, a, gi, gj, kz, nbx);
-                        store_u(a.u_out, (size_t)F_BY * a.uf, a, gi, gj, kz, nby);
-                    }
                     // on the walls RU, RV, RW, TT, BZ are rewritten by BCON below
-                    store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, kz, nu);
-                    store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, kz, nv);
-                    store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, kz, nw);
-                    store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, kz, nt);
-                    if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, kz, nbz);
+                    double* const pl = a.u_out + (size_t)kz * a.uz;
+                    if (MAG)
+                        store_cell<8>(pl, a.uf, ucol, hc, {F_RO, F_BX, F_BY, F_RU, F_RV, F_RW, F_TT, F_BZ},
+                                      {nr, nbx, nby, nu, nv, nw, nt, nbz});
+                    else
+                        store_cell<5>(pl, a.uf, ucol, hc, {F_RO, F_RU, F_RV, F_RW, F_TT}, {nr, nu, nv, nw, nt});
                     // ---- Z for the next stage: Z = U + ZETA*DT*F (loops 190-260, 390-460).
                     //      On the walls only RO, BX, BY are ever read back.
                     if (STAGE < 3) {
@@ -929,11 +967,11 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                     }
                     const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : w0_bz;
                     if (zok) {
-                        store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, 1, ru_w);
-                        store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, 1, rv_w);
-                        store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, 1, 0.0);
-                        store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, 1, tt_w);
-                        if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, 1, bz_w);
+                        double* const pl = a.u_out + a.uz;
+                        if (MAG)
+                            store_cell<5>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT, F_BZ}, {ru_w, rv_w, 0.0, tt_w, bz_w});
+                        else
+                            store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
                     if (STAGE == 3)
                         cfl_acc_direct<MAG>(cfa, s, m, gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
@@ -951,11 +989,11 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                     const double tt_w = (s.izcon == 0) ? s.tb : C43 * h1_tt - C13 * h2_tt + s.bot_flux;
                     const double bz_w = (MAG && s.ibcon == 0) ? 0.0 : nbz;
                     if (zok) {
-                        store_u(a.u_out, (size_t)F_RU * a.uf, a, gi, gj, kz, ru_w);
-                        store_u(a.u_out, (size_t)F_RV * a.uf, a, gi, gj, kz, rv_w);
-                        store_u(a.u_out, (size_t)F_RW * a.uf, a, gi, gj, kz, 0.0);
-                        store_u(a.u_out, (size_t)F_TT * a.uf, a, gi, gj, kz, tt_w);
-                        if (MAG) store_u(a.u_out, (size_t)F_BZ * a.uf, a, gi, gj, kz, bz_w);
+                        double* const pl = a.u_out + (size_t)kz * a.uz;
+                        if (MAG)
+                            store_cell<5>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT, F_BZ}, {ru_w, rv_w, 0.0, tt_w, bz_w});
+                        else
+                            store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
                     if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
                 }
