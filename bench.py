@@ -192,7 +192,7 @@ def main():
     ap.add_argument("--mode", choices=["fast", "exact"], default="fast")
     ap.add_argument("--grid", type=str, default=None, help="override NPXxNPYxNPZ (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-npz", type=int, default=SAMPLE_NPZ)
     args = ap.parse_args()
     if args.warmup < 3:
