@@ -52,11 +52,19 @@ extern "C" {
 #define MHD3D_ERR_TIMEOUT      6  /* a bounded device-side wait gave up */
 #define MHD3D_ERR_NOMEM        7  /* device allocation failed */
 
-/* Arithmetic modes of the FP64 path. */
-#define MHD3D_MODE_EXACT 0   /* reference operation order, no FMA contraction:
-                                bit-equal to the CPU restatement (+0 == -0) */
-#define MHD3D_MODE_FAST  1   /* FMA contraction and pre-multiplied metric
+/* Arithmetic modes. */
+#define MHD3D_MODE_EXACT 0   /* FP64, reference operation order, no FMA
+                                contraction: bit-equal to the CPU restatement
+                                (+0 == -0) */
+#define MHD3D_MODE_FAST  1   /* FP64, FMA contraction and pre-multiplied metric
                                 products; within 1e-11 of EXACT after 10 steps */
+#define MHD3D_MODE_FP32  2   /* FP32 state held as perturbations from FP64
+                                background profiles (the horizontal means of
+                                TT, RO, BX, BY, BZ at upload), FP32 arithmetic,
+                                FP64 metrics and CFL reduction.  No counterpart
+                                in the reference; its per-field error against
+                                the FP64 path is measured by the tests.
+                                mhd3d_bcon is not available in this mode. */
 
 /*
  * Scalars of the COMMON blocks the step reads.  The host fills them exactly
@@ -68,7 +76,7 @@ typedef struct mhd3d_params {
     int32_t npx, npy, npz;      /* NPX,NPY,NPZ (3dmhdparam.f:13)                 */
     int32_t lmag, lrot;         /* LMAG, LROT (3dmhdparam.f:8)                    */
     int32_t izcon, itcon, ibcon;/* IZC, ITC, IBC (COMMON/BCT, 3dmhdparam.f:27)   */
-    int32_t mode;               /* MHD3D_MODE_EXACT or MHD3D_MODE_FAST            */
+    int32_t mode;               /* MHD3D_MODE_EXACT, _FAST or _FP32               */
     int32_t reserved0;
     /* COMMON/GRID (DD is a STEP-local scratch there and is not passed) */
     double c13, c23, c43;

@@ -39,6 +39,14 @@ struct Handle {
     int ntx = 0, zlen = 0, nchunks = 0;
     bool dt_valid = false;
     unsigned long long w4key = ~0ull;   // key of min over cells of W4 (MHD), else ~0
+    // FP32 form: the buffers above hold floats; background profiles
+    bool f32 = false;
+    double* bgd = nullptr;        // 5 x NZ: RHOb, Tb, BXb, BYb, BZb (FP64)
+    float* bg32 = nullptr;        // 2 x NZ: RHOb, Tb (FP32)
+    PlaneBg* pb = nullptr;        // per interior plane
+    std::vector<double> faz_h, fbz_h, fcz_h;   // host copies of the z stencil factors
+    double top_lin = 0.0, top_tb = 0.0;
+    float t_top_fix = 0.f, t_top_fix4 = 0.f, t_top_flux = 0.f, t_bot = 0.f;
     cudaStream_t own = nullptr;   // the handle's stream; st may be a caller's
     // asynchronous stepping: state at the last sync and steps enqueued since
     int nit_base = 0, cur_base = 0, pending = 0;
@@ -100,6 +108,75 @@ __global__ void k_pack_interior(const double* __restrict__ f, double* __restrict
         double v = 0.0;
         if (I > 0 && I < NX - 1 && J > 0 && J < NY - 1 && K > 0 && K < NZ - 1)
             v = f[(size_t)(K - 1) * zz + (size_t)(J - 1) * zpitch + (I - 1)];
+        fort[q] = v;
+    }
+}
+
+// horizontal mean of one Fortran (NX,NY,NZ) field per plane K over the
+// interior I=2..NX-1, J=2..NY-1, FP64, fixed summation order (one block per K)
+__global__ void k_hmean(const double* __restrict__ fort, double* __restrict__ mean, int npx, int npy)
+{
+    const int NX = npx + 2, NY = npy + 2;
+    const int K = blockIdx.x;
+    const double* pl = fort + (size_t)K * NX * NY;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < npx * npy; q += blockDim.x) {
+        const int i = q % npx, j = q / npx;
+        acc += pl[(size_t)(j + 1) * NX + (i + 1)];
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) mean[K] = red[0] / ((double)npx * (double)npy);
+}
+
+// Fortran (NX,NY,NZ) FP64 -> both FP32 U buffers as perturbations from bg(K)
+// (bg may be null: no background), halos refreshed from the interior
+__global__ void k_unpack32(const double* __restrict__ fort, const double* __restrict__ bg, float* __restrict__ u0,
+                           float* __restrict__ u1, int npx, int npy, int npz, int upitch, size_t uz)
+{
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        const int Is = I == 0 ? npx : (I == NX - 1 ? 1 : I);
+        const int Js = J == 0 ? npy : (J == NY - 1 ? 1 : J);
+        double v = fort[(size_t)Is + (size_t)NX * ((size_t)Js + (size_t)NY * K)];
+        if (bg) v -= bg[K];
+        const size_t d = (size_t)K * uz + (size_t)J * upitch + I;
+        u0[d] = (float)v;
+        u1[d] = (float)v;
+    }
+}
+
+// FP32 U layout -> Fortran (NX,NY,NZ) FP64 full values
+__global__ void k_pack32(const float* __restrict__ u, const double* __restrict__ bg, double* __restrict__ fort,
+                         int npx, int npy, int npz, int upitch, size_t uz)
+{
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        const double v = (double)u[(size_t)K * uz + (size_t)J * upitch + I];
+        fort[q] = bg ? bg[K] + v : v;
+    }
+}
+
+// FP32 Z layout (interior) -> Fortran (NX,NY,NZ) FP64, zeros outside
+__global__ void k_pack_interior32(const float* __restrict__ f, double* __restrict__ fort, int npx, int npy, int npz,
+                                  int zpitch, size_t zz)
+{
+    const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
+    const size_t n = (size_t)NX * NY * NZ;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), K = (int)(q / ((size_t)NX * NY));
+        double v = 0.0;
+        if (I > 0 && I < NX - 1 && J > 0 && J < NY - 1 && K > 0 && K < NZ - 1)
+            v = (double)f[(size_t)(K - 1) * zz + (size_t)(J - 1) * zpitch + (I - 1)];
         fort[q] = v;
     }
 }
@@ -182,12 +259,48 @@ StageArgs make_args(Handle* h)
     return a;
 }
 
+StageArgs32 make_args32(Handle* h)
+{
+    StageArgs32 a{};
+    a.map_u = h->map_u[h->cur];
+    a.map_z = h->map_z;
+    a.u_in = reinterpret_cast<const float*>(h->ubuf[h->cur]);
+    a.u_out = reinterpret_cast<float*>(h->ubuf[h->cur ^ 1]);
+    a.z = reinterpret_cast<float*>(h->z);
+    a.f_out = reinterpret_cast<float*>(h->fout);
+    a.ctl = h->ctl;
+    a.acc = h->acc;
+    a.m = h->m;
+    a.s = h->s;
+    const size_t NZ = (size_t)h->p.npz + 2;
+    a.rob = h->bg32;
+    a.ttb = h->bg32 + NZ;
+    a.bgd = h->bgd;
+    a.pb = h->pb;
+    a.top_lin = h->top_lin;
+    a.top_tb = h->top_tb;
+    a.t_top_fix = h->t_top_fix;
+    a.t_top_fix4 = h->t_top_fix4;
+    a.t_top_flux = h->t_top_flux;
+    a.t_bot = h->t_bot;
+    a.uf = h->uf;
+    a.uz = h->uz;
+    a.zf = h->zf;
+    a.zz = h->zz;
+    a.upitch = h->upitch;
+    a.zpitch = h->zpitch;
+    a.ntx = h->ntx;
+    a.zlen = h->zlen;
+    a.nchunks = h->nchunks;
+    return a;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// 4-D tiled TMA map (x, y, z, field) of a double array, no swizzle, zero fill
-int make_map(CUtensorMap* map, double* base, const cuuint64_t dims[4], const cuuint32_t box[4])
+// 4-D tiled TMA map (x, y, z, field) of a double or float array, no swizzle, zero fill
+int make_map(CUtensorMap* map, void* base, const cuuint64_t dims[4], const cuuint32_t box[4], bool f32 = false)
 {
     static EncodeTiledFn enc = nullptr;
     if (!enc) {
@@ -197,9 +310,11 @@ int make_map(CUtensorMap* map, double* base, const cuuint64_t dims[4], const cuu
             return MHD3D_ERR_CUDA;
         enc = reinterpret_cast<EncodeTiledFn>(fn);
     }
-    const cuuint64_t strides[3] = {dims[0] * 8, dims[0] * dims[1] * 8, dims[0] * dims[1] * dims[2] * 8};
+    const cuuint64_t es = f32 ? 4 : 8;
+    const cuuint64_t strides[3] = {dims[0] * es, dims[0] * dims[1] * es, dims[0] * dims[1] * dims[2] * es};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr,
+    CUresult r = enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                     strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -216,6 +331,7 @@ cudaError_t launch_stage(Handle* h, int stage, const StageArgs& a)
 
 cudaError_t launch_cfl(Handle* h, const StageArgs& a)
 {
+    if (h->f32) return f32::launch_cfl(make_args32(h), h->st);
     return h->p.mode == MHD3D_MODE_FAST ? fast::launch_cfl(a, h->st) : exact::launch_cfl(a, h->st);
 }
 
@@ -225,7 +341,7 @@ int validate(const mhd3d_params* p)
     if (p->npx < 2 || p->npy < 2 || p->npz < 4) return MHD3D_ERR_ARG;
     if (p->izcon != 0 && p->izcon != 1) return MHD3D_ERR_ARG;
     if (p->itcon < 0 || p->itcon > 4 || p->itcon == 2) return MHD3D_ERR_ARG;
-    if (p->mode != MHD3D_MODE_EXACT && p->mode != MHD3D_MODE_FAST) return MHD3D_ERR_ARG;
+    if (p->mode != MHD3D_MODE_EXACT && p->mode != MHD3D_MODE_FAST && p->mode != MHD3D_MODE_FP32) return MHD3D_ERR_ARG;
     if ((size_t)(p->npx + 2) * (p->npy + 2) * (p->npz + 2) > ((size_t)1 << 40)) return MHD3D_ERR_ARG;
     return MHD3D_OK;
 }
@@ -240,6 +356,9 @@ int destroy(Handle* h)
     cudaFree(h->stage);
     cudaFree(h->fout);
     cudaFree(h->met);
+    cudaFree(h->bgd);
+    cudaFree(h->bg32);
+    cudaFree(h->pb);
     cudaFree(h->ctl);
     cudaFree(h->acc);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -266,20 +385,24 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     const int npx = p->npx, npy = p->npy, npz = p->npz;
     const int NX = npx + 2, NY = npy + 2, NZ = npz + 2;
     h->nf = p->lmag ? 8 : 5;
-    // U: the Fortran index space (halos, ghost planes), rows padded to even
-    // length and to at least one TMA box; Z: interior cells only
-    h->upitch = (NX + 1) / 2 * 2;
-    if (h->upitch < BW) h->upitch = BW;
-    h->urows = NY < BH ? BH : NY;
+    h->f32 = p->mode == MHD3D_MODE_FP32;
+    // U: the Fortran index space (halos, ghost planes), rows padded to 16
+    // bytes and to at least one TMA box; Z: interior cells only
+    const int ealign = h->f32 ? 4 : 2;                 // elements per 16 bytes
+    const int bw = h->f32 ? BW32 : BW, bh = h->f32 ? BH32 : BH, ty = h->f32 ? TY32 : TY;
+    h->upitch = (NX + ealign - 1) / ealign * ealign;
+    if (h->upitch < bw) h->upitch = bw;
+    h->urows = NY < bh ? bh : NY;
     h->uz = (size_t)h->urows * h->upitch;
     h->uf = (size_t)NZ * h->uz;
-    h->zpitch = (npx + 1) / 2 * 2;
+    h->zpitch = (npx + ealign - 1) / ealign * ealign;
     if (h->zpitch < TX) h->zpitch = TX;
-    h->zrows = npy < TY ? TY : npy;
+    h->zrows = npy < ty ? ty : npy;
     h->zz = (size_t)h->zrows * h->zpitch;
     h->zf = (size_t)npz * h->zz;
-    const size_t ubytes = sizeof(double) * h->nf * h->uf;
-    const size_t zbytes = sizeof(double) * h->nf * h->zf;
+    const size_t esize = h->f32 ? sizeof(float) : sizeof(double);
+    const size_t ubytes = esize * h->nf * h->uf;
+    const size_t zbytes = esize * h->nf * h->zf;
     CK(cudaMalloc(&h->ubuf[0], ubytes));
     CK(cudaMalloc(&h->ubuf[1], ubytes));
     CK(cudaMalloc(&h->z, zbytes));
@@ -288,15 +411,23 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     CK(cudaMemset(h->z, 0, zbytes));
     {
         const cuuint64_t du[4] = {(cuuint64_t)h->upitch, (cuuint64_t)h->urows, (cuuint64_t)NZ, (cuuint64_t)h->nf};
-        const cuuint32_t bu[4] = {BW, BH, 1, (cuuint32_t)h->nf};
+        const cuuint32_t bu[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, (cuuint32_t)h->nf};
         for (int b = 0; b < 2; ++b) {
-            int st2 = make_map(&h->map_u[b], h->ubuf[b], du, bu);
+            int st2 = make_map(&h->map_u[b], h->ubuf[b], du, bu, h->f32);
             if (st2) return st2;
         }
         const cuuint64_t dz[4] = {(cuuint64_t)h->zpitch, (cuuint64_t)h->zrows, (cuuint64_t)npz, (cuuint64_t)h->nf};
-        const cuuint32_t bz[4] = {TX, TY, 1, (cuuint32_t)h->nf};
-        int st3 = make_map(&h->map_z, h->z, dz, bz);
+        const cuuint32_t bz[4] = {TX, (cuuint32_t)ty, 1, (cuuint32_t)h->nf};
+        int st3 = make_map(&h->map_z, h->z, dz, bz, h->f32);
         if (st3) return st3;
+    }
+    if (h->f32) {
+        CK(cudaMalloc(&h->bgd, sizeof(double) * 5 * NZ));
+        CK(cudaMemset(h->bgd, 0, sizeof(double) * 5 * NZ));
+        CK(cudaMalloc(&h->bg32, sizeof(float) * 2 * NZ));
+        CK(cudaMemset(h->bg32, 0, sizeof(float) * 2 * NZ));
+        CK(cudaMalloc(&h->pb, sizeof(PlaneBg) * npz));
+        CK(cudaMemset(h->pb, 0, sizeof(PlaneBg) * npz));
     }
     CK(cudaMalloc(&h->stage, sizeof(double) * (size_t)NX * NY * NZ));
     CK(cudaMalloc(&h->ctl, sizeof(Control)));
@@ -384,6 +515,9 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
         const double f_lo = 0.5 * dlo * dlo * p->rm, f_hi = 0.5 * dhi * dhi * p->rm;
         h->w4key = std::min(key_of(f_lo), key_of(f_hi));
     }
+    h->faz_h.assign(hm + offs[19], hm + offs[19] + NZ);
+    h->fbz_h.assign(hm + offs[20], hm + offs[20] + NZ);
+    h->fcz_h.assign(hm + offs[21], hm + offs[21] + NZ);
     CK(cudaMalloc(&h->met, sizeof(double) * tot));
     CK(cudaMemcpy(h->met, hm, sizeof(double) * tot, cudaMemcpyHostToDevice));
     h->m.dxxdx = h->met + offs[0];
@@ -460,6 +594,79 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     return MHD3D_OK;
 }
 
+// background index of a field in the FP32 form (-1: stored whole)
+int bg_index(int fi)
+{
+    switch (fi) {
+        case F_RO: return 0;
+        case F_TT: return 1;
+        case F_BX: return 2;
+        case F_BY: return 3;
+        case F_BZ: return 4;
+        default: return -1;
+    }
+}
+
+// FP32 form: per-plane background terms from the FP64 horizontal means
+int set_background(Handle* h)
+{
+    const int npz = h->p.npz, NZ = npz + 2;
+    std::vector<double> b(5 * (size_t)NZ);
+    CK(cudaMemcpyAsync(b.data(), h->bgd, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const double* R = b.data();
+    const double* T = R + NZ;
+    const double* B[3] = {R + 2 * NZ, R + 3 * NZ, R + 4 * NZ};
+    std::vector<float> b32(2 * (size_t)NZ);
+    for (int u = 0; u < NZ; ++u) {
+        b32[u] = (float)R[u];
+        b32[NZ + u] = (float)T[u];
+    }
+    const double grav = h->p.grav;
+    std::vector<PlaneBg> pb(npz);
+    for (int k = 0; k < npz; ++k) {
+        const int u = k + 1;   // U plane of interior plane k (Fortran K = k+2)
+        const double az = h->faz_h[u], bzq = h->fbz_h[u], czq = h->fcz_h[u];
+        PlaneBg& q = pb[k];
+        const double tz = T[u + 1] - T[u - 1];
+        q.tz = (float)tz;
+        q.tlz = (float)(tz * bzq + (T[u + 1] + T[u - 1] - 2.0 * T[u]) * czq);
+        q.fw = (float)(grav * R[u] - (R[u + 1] * T[u + 1] - R[u - 1] * T[u - 1]) * az);
+        float* bc[3] = {&q.bx, &q.by, &q.bz};
+        float* bd[3] = {&q.bxz, &q.byz, &q.bzz};
+        float* bl[3] = {&q.bxlz, &q.bylz, &q.bzlz};
+        for (int c = 0; c < 3; ++c) {
+            const double* Bc = B[c];
+            *bc[c] = (float)Bc[u];
+            *bd[c] = (float)(Bc[u + 1] - Bc[u - 1]);
+            double lz;
+            // BX and BY take the one-sided second difference on the walls (as in the kernel)
+            if (c < 2 && k == 0)
+                lz = (-3.0 * Bc[u] + 4.0 * Bc[u + 1] - Bc[u + 2]) * bzq
+                   + (2.0 * Bc[u] - 5.0 * Bc[u + 1] + 4.0 * Bc[u + 2] - Bc[u + 3]) * czq;
+            else if (c < 2 && k == npz - 1)
+                lz = (3.0 * Bc[u] - 4.0 * Bc[u - 1] + Bc[u - 2]) * bzq
+                   + (2.0 * Bc[u] - 5.0 * Bc[u - 1] + 4.0 * Bc[u - 2] - Bc[u - 3]) * czq;
+            else
+                lz = (Bc[u + 1] - Bc[u - 1]) * bzq + (Bc[u + 1] + Bc[u - 1] - 2.0 * Bc[u]) * czq;
+            *bl[c] = (float)lz;
+        }
+    }
+    // wall temperatures in perturbation form (BCON 3dmhdsub.f:2833-2868, 2917-2941)
+    const double C13 = h->p.c13, C43 = h->p.c43;
+    h->top_tb = T[1];
+    h->top_lin = C43 * T[2] - C13 * T[3] - T[1];
+    h->t_top_fix = (float)(1.0 - T[1]);
+    h->t_top_fix4 = (float)((1.0 - h->p.tp) - T[1]);
+    h->t_top_flux = (float)(h->top_lin - h->s.top_flux);
+    h->t_bot = h->p.izcon == 0 ? (float)(h->p.tb - T[npz])
+                               : (float)(C43 * T[npz - 1] - C13 * T[npz - 2] + h->s.bot_flux - T[npz]);
+    CK(cudaMemcpyAsync(h->bg32, b32.data(), sizeof(float) * b32.size(), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->pb, pb.data(), sizeof(PlaneBg) * pb.size(), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
 int upload(Handle* h, const double* const f[8])
 {
     CK(cudaSetDevice(h->dev));
@@ -469,11 +676,25 @@ int upload(Handle* h, const double* const f[8])
         if (!f[i]) return MHD3D_ERR_ARG;
     for (int fi = 0; fi < h->nf; ++fi) {
         CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyHostToDevice, h->st));
-        k_unpack<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, h->ubuf[0] + (size_t)fi * h->uf,
-                                                     h->ubuf[1] + (size_t)fi * h->uf, npx, npy, npz, h->upitch, h->uz);
+        if (h->f32) {
+            const int bi = bg_index(fi);
+            double* bg = bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr;
+            if (bg) k_hmean<<<npz + 2, 256, 0, h->st>>>(h->stage, bg, npx, npy);
+            float* u0 = reinterpret_cast<float*>(h->ubuf[0]) + (size_t)fi * h->uf;
+            float* u1 = reinterpret_cast<float*>(h->ubuf[1]) + (size_t)fi * h->uf;
+            k_unpack32<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, bg, u0, u1, npx, npy, npz, h->upitch, h->uz);
+        } else {
+            k_unpack<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, h->ubuf[0] + (size_t)fi * h->uf,
+                                                         h->ubuf[1] + (size_t)fi * h->uf, npx, npy, npz, h->upitch,
+                                                         h->uz);
+        }
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->st));
+    if (h->f32) {
+        int st = set_background(h);
+        if (st) return st;
+    }
     h->dt_valid = false;
     h->cur_base = h->cur;
     h->pending = 0;
@@ -487,8 +708,15 @@ int download(Handle* h, double* const f[8])
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
     for (int fi = 0; fi < h->nf; ++fi) {
         if (!f[fi]) continue;
-        k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->uf, h->stage, npx, npy, npz,
-                                                   h->upitch, h->uz);
+        if (h->f32) {
+            const int bi = bg_index(fi);
+            k_pack32<<<grid_for(nfort), 256, 0, h->st>>>(
+                reinterpret_cast<const float*>(h->ubuf[h->cur]) + (size_t)fi * h->uf,
+                bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr, h->stage, npx, npy, npz, h->upitch, h->uz);
+        } else {
+            k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->uf, h->stage, npx, npy,
+                                                       npz, h->upitch, h->uz);
+        }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
     }
@@ -539,15 +767,23 @@ int step_async(Handle* h, int n)
     int cur = h->cur_base ^ (h->pending & 1);
     for (int s = 0; s < n; ++s) {
         for (int stg = 1; stg <= 3; ++stg) {
-            StageArgs a = make_args(h);
-            a.map_u = h->map_u[cur];
-            a.u_in = h->ubuf[cur];
-            a.u_out = h->ubuf[cur ^ 1];
             if (h->prof) {
                 int st = record_event(h, stg - 1);
                 if (st) return st;
             }
-            CK(launch_stage(h, stg, a));
+            if (h->f32) {
+                StageArgs32 a = make_args32(h);
+                a.map_u = h->map_u[cur];
+                a.u_in = reinterpret_cast<const float*>(h->ubuf[cur]);
+                a.u_out = reinterpret_cast<float*>(h->ubuf[cur ^ 1]);
+                CK(f32::launch_stage(stg, a, h->st));
+            } else {
+                StageArgs a = make_args(h);
+                a.map_u = h->map_u[cur];
+                a.u_in = h->ubuf[cur];
+                a.u_out = h->ubuf[cur ^ 1];
+                CK(launch_stage(h, stg, a));
+            }
             if (h->prof) {
                 int st = record_event(h, -1);
                 if (st) return st;
@@ -594,15 +830,23 @@ int fluxes(Handle* h, double* const out[8])
 {
     CK(cudaSetDevice(h->dev));
     if (int st = settle(h)) return st;
-    if (!h->fout) CK(cudaMalloc(&h->fout, sizeof(double) * h->nf * h->zf));
-    StageArgs a = make_args(h);
-    CK(launch_stage(h, 0, a));
+    if (!h->fout) CK(cudaMalloc(&h->fout, (h->f32 ? sizeof(float) : sizeof(double)) * h->nf * h->zf));
+    if (h->f32) {
+        CK(f32::launch_stage(0, make_args32(h), h->st));
+    } else {
+        StageArgs a = make_args(h);
+        CK(launch_stage(h, 0, a));
+    }
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
     for (int fi = 0; fi < h->nf; ++fi) {
         if (!out[fi]) continue;
-        k_pack_interior<<<grid_for(nfort), 256, 0, h->st>>>(h->fout + (size_t)fi * h->zf, h->stage, npx, npy, npz,
-                                                            h->zpitch, h->zz);
+        if (h->f32)
+            k_pack_interior32<<<grid_for(nfort), 256, 0, h->st>>>(
+                reinterpret_cast<const float*>(h->fout) + (size_t)fi * h->zf, h->stage, npx, npy, npz, h->zpitch, h->zz);
+        else
+            k_pack_interior<<<grid_for(nfort), 256, 0, h->st>>>(h->fout + (size_t)fi * h->zf, h->stage, npx, npy,
+                                                                npz, h->zpitch, h->zz);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
     }
@@ -745,6 +989,7 @@ int mhd3d_bcon(void* handle)
     Handle* h = static_cast<Handle*>(handle);
     CK(cudaSetDevice(h->dev));
     if (int st = settle(h)) return st;
+    if (h->f32) return MHD3D_ERR_ARG;
     StageArgs a = make_args(h);
     CK(h->p.mode == MHD3D_MODE_FAST ? fast::launch_bcon(a, h->st) : exact::launch_bcon(a, h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -752,6 +997,6 @@ int mhd3d_bcon(void* handle)
     return MHD3D_OK;
 }
 
-const char* mhd3d_version(void) { return "mhd3d-b200 0.1 (sm_100a, FP64)"; }
+const char* mhd3d_version(void) { return "mhd3d-b200 0.2 (sm_100a, FP64 exact/FMA, FP32 perturbation form)"; }
 
 }  // extern "C"

@@ -110,6 +110,54 @@ struct StageArgs {
     int nchunks;
 };
 
+// ---- FP32 form ----------------------------------------------------------
+// The state is held in FP32 as perturbations from FP64 background profiles
+// (horizontal means of TT, RO, BX, BY, BZ per plane, taken when the state is
+// uploaded; the momenta have none).  Every term of the right-hand side that
+// involves a z difference of a background is formed on the host in FP64 and
+// rounded once to FP32 per plane (PlaneBg); x and y differences of a
+// background vanish, so the FP32 arithmetic only ever sees perturbation-sized
+// differences.  Metrics stay FP64 in memory; the CFL reduction is FP64.
+#ifndef MHD3D_TY32
+#define MHD3D_TY32 4
+#endif
+constexpr int TY32 = MHD3D_TY32;        // tile rows of the FP32 kernel
+constexpr int NT32 = TX * TY32;
+constexpr int BW32 = 36;                // TMA box row: x0-1 .. x0+34 (36 floats = 144 B, a 16-B multiple)
+constexpr int BH32 = TY32 + 2;
+constexpr int BSLOT32 = BW32 * BH32;
+
+struct PlaneBg {
+    float tz;                 // Tb(K+1)-Tb(K-1)
+    float tlz;                // z part of the Laplacian of Tb: tz*BZQ(K) + (Tb(K+1)+Tb(K-1)-2Tb(K))*CZQ(K)
+    float fw;                 // GRAV*RHOb(K) - (Pb(K+1)-Pb(K-1))*AZ(K), Pb=RHOb*Tb
+    float bx, by, bz;         // Bb(K)
+    float bxz, byz, bzz;      // Bb(K+1)-Bb(K-1)
+    float bxlz, bylz, bzlz;   // z part of the Laplacian of Bb (one-sided on the walls, like B's)
+};
+
+struct StageArgs32 {
+    CUtensorMap map_u;
+    CUtensorMap map_z;
+    const float* u_in;
+    float* u_out;
+    float* z;
+    float* f_out;
+    Control* ctl;
+    Accum* acc;
+    Metrics m;
+    Scalars s;
+    const float* rob;         // RHOb at every U plane (Fortran K=1..NZ)
+    const float* ttb;         // Tb at every U plane
+    const double* bgd;        // FP64 backgrounds: RHOb, Tb, BXb, BYb, BZb, NZ values each
+    const PlaneBg* pb;        // per interior plane
+    double top_lin, top_tb;   // C43*Tb(3)-C13*Tb(4)-Tb(2) and Tb(2): top-wall temperature in perturbation form
+    float t_top_fix, t_top_fix4, t_top_flux, t_bot;   // wall T' constants (ITC 0/2/4, ITC=4 left half, ITC=1; IZC)
+    size_t uf, uz, zf, zz;
+    int upitch, zpitch;
+    int ntx, zlen, nchunks;
+};
+
 // order-preserving map double -> uint64 and back
 __host__ __device__ inline unsigned long long key_of(double x)
 {
@@ -138,6 +186,12 @@ size_t stage_smem_bytes(int lmag);
 cudaError_t launch_stage(int stage, const StageArgs& a, cudaStream_t st);
 cudaError_t launch_cfl(const StageArgs& a, cudaStream_t st);
 cudaError_t launch_bcon(const StageArgs& a, cudaStream_t st);
+}
+// FP32 form (FMA contraction, FP64 CFL reduction)
+namespace f32 {
+size_t stage_smem_bytes(int lmag);
+cudaError_t launch_stage(int stage, const StageArgs32& a, cudaStream_t st);
+cudaError_t launch_cfl(const StageArgs32& a, cudaStream_t st);
 }
 
 }  // namespace mhd3d

@@ -11,7 +11,7 @@ module mhd3d_gpu
   integer(c_int), parameter :: MHD3D_OK = 0, MHD3D_ERR_ARG = 1, MHD3D_ERR_CUDA = 2, &
        MHD3D_ERR_NONFINITE = 3, MHD3D_ERR_DT_SMALL = 4, MHD3D_ERR_NO_DEVICE = 5, &
        MHD3D_ERR_TIMEOUT = 6, MHD3D_ERR_NOMEM = 7
-  integer(c_int), parameter :: MHD3D_MODE_EXACT = 0, MHD3D_MODE_FAST = 1
+  integer(c_int), parameter :: MHD3D_MODE_EXACT = 0, MHD3D_MODE_FAST = 1, MHD3D_MODE_FP32 = 2
 
   type, bind(C) :: mhd3d_params
      integer(c_int32_t) :: npx, npy, npz

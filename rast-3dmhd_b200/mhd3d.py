@@ -26,6 +26,7 @@ FLUXES = ("fu", "fv", "fw", "fr", "ft", "ww1", "ww2", "ww3")
 
 MODE_EXACT = 0
 MODE_FAST = 1
+MODE_FP32 = 2
 
 GRID_UNIFORM, GRID_ARCTAN, GRID_DIP, GRID_TANH_Z = 0, 1, 2, 3
 
