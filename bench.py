@@ -189,7 +189,8 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--mode", choices=["fast", "exact", "fp32"], default="fast",
+                    help="fast: FP64 with FMA (default); exact: FP64 reference rounding; fp32: FP32 form")
     ap.add_argument("--grid", type=str, default=None, help="override NPXxNPYxNPZ (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -227,7 +228,8 @@ def main():
     setup = mhd3d.make_setup(cfg)
     cells = w["npx"] * w["npy"] * w["npz"]
     nf = 8 if cfg.lmag else 5
-    mode = mhd3d.MODE_FAST if args.mode == "fast" else mhd3d.MODE_EXACT
+    mode = {"fast": mhd3d.MODE_FAST, "exact": mhd3d.MODE_EXACT, "fp32": mhd3d.MODE_FP32}[args.mode]
+    word = 4 if args.mode == "fp32" else 8
     sim = mhd3d.GpuSim(setup, mode=mode)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
@@ -272,14 +274,14 @@ def main():
     peaks, peak_src = measured_peaks()
     launches = sum(stage_n)
     kernel_ms = sum(stage_ms) / max(launches, 1)
-    bytes_per_launch = 10 * nf * 8 * cells / 3.0
+    bytes_per_launch = 10 * nf * word * cells / 3.0
     achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        key = "mhd_fp64_" + args.mode
+        key = "mhd_fp32" if args.mode == "fp32" else "mhd_fp64_" + args.mode
         if key in tj:
             traffic = tj[key]["dram_bytes_per_cell_per_launch"] * cells
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -339,7 +341,7 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.mode == "fp32" else "f64",
                 "data": "synthetic: rotating MHD polytrope from the host mirror of STATIC/TUBE model 4/RAN2",
                 "config": {"workload": WORKLOAD_NAME, "grid": [w["npx"], w["npy"], w["npz"]],
                            "mode": args.mode, "fields": nf,

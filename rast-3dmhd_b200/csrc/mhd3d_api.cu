@@ -45,6 +45,9 @@ struct Handle {
     float* bg32 = nullptr;        // 2 x NZ: RHOb, Tb (FP32)
     PlaneBg* pb = nullptr;        // per interior plane
     std::vector<double> faz_h, fbz_h, fcz_h;   // host copies of the z stencil factors
+    std::vector<double> rka_h, dka_h, ddz_h;   // and of RKAPA, DKAPA, DDZ
+    ColC* cxy = nullptr;                       // FP32 column constants: NX in x, then NY in y
+    Scalars32 s32{};
     double top_lin = 0.0, top_tb = 0.0;
     float t_top_fix = 0.f, t_top_fix4 = 0.f, t_top_flux = 0.f, t_bot = 0.f;
     cudaStream_t own = nullptr;   // the handle's stream; st may be a caller's
@@ -277,6 +280,9 @@ StageArgs32 make_args32(Handle* h)
     a.ttb = h->bg32 + NZ;
     a.bgd = h->bgd;
     a.pb = h->pb;
+    a.cx = h->cxy;
+    a.cy = h->cxy + (h->p.npx + 2);
+    a.s32 = h->s32;
     a.top_lin = h->top_lin;
     a.top_tb = h->top_tb;
     a.t_top_fix = h->t_top_fix;
@@ -359,6 +365,7 @@ int destroy(Handle* h)
     cudaFree(h->bgd);
     cudaFree(h->bg32);
     cudaFree(h->pb);
+    cudaFree(h->cxy);
     cudaFree(h->ctl);
     cudaFree(h->acc);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -518,6 +525,31 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     h->faz_h.assign(hm + offs[19], hm + offs[19] + NZ);
     h->fbz_h.assign(hm + offs[20], hm + offs[20] + NZ);
     h->fcz_h.assign(hm + offs[21], hm + offs[21] + NZ);
+    h->rka_h.assign(src[9], src[9] + NZ);
+    h->dka_h.assign(src[10], src[10] + NZ);
+    h->ddz_h.assign(src[8], src[8] + NZ);
+    if (h->f32) {
+        // column constants of the FP32 kernel
+        std::vector<ColC> cc((size_t)NX + NY);
+        for (int i = 0; i < NX; ++i) {
+            ColC& c = cc[i];
+            c.a = (float)hm[offs[13] + i];
+            c.b = (float)hm[offs[14] + i];
+            c.c = (float)hm[offs[15] + i];
+            c.rdd = (float)(1.0 / src[2][i]);
+            c.dd = (float)src[2][i];
+        }
+        for (int j = 0; j < NY; ++j) {
+            ColC& c = cc[(size_t)NX + j];
+            c.a = (float)hm[offs[16] + j];
+            c.b = (float)hm[offs[17] + j];
+            c.c = (float)hm[offs[18] + j];
+            c.rdd = (float)(1.0 / src[5][j]);
+            c.dd = (float)src[5][j];
+        }
+        CK(cudaMalloc(&h->cxy, sizeof(ColC) * cc.size()));
+        CK(cudaMemcpy(h->cxy, cc.data(), sizeof(ColC) * cc.size(), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&h->met, sizeof(double) * tot));
     CK(cudaMemcpy(h->met, hm, sizeof(double) * tot, cudaMemcpyHostToDevice));
     h->m.dxxdx = h->met + offs[0];
@@ -561,6 +593,14 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     s.tmp_13 = p->c13 * p->ore;
     s.tmp_m = p->obeta * p->orm * p->ocv;
     s.cw3 = 0.375 * p->re;
+    {
+        Scalars32& f = h->s32;
+        f.grav = (float)p->grav; f.ore = (float)p->ore; f.c13 = (float)p->c13; f.c43 = (float)p->c43;
+        f.tmp13 = (float)s.tmp_13; f.tmpa = (float)s.tmp_a; f.tmpb = (float)s.tmp_b; f.tmpc = (float)s.tmp_cond;
+        f.ocv = (float)p->ocv; f.omx = (float)p->omx; f.omz = (float)p->omz; f.orm = (float)p->orm;
+        f.obeta = (float)p->obeta; f.tmpm = (float)s.tmp_m; f.ogamma = (float)(1.0 / p->gamma);
+        f.gamma = (float)p->gamma; f.cw3 = (float)s.cw3;
+    }
     s.tb = p->tb; s.tp = p->tp; s.tc = p->tc; s.hh = p->hh;
     const double dzs = (double)(1.0f / (float)(npz - 1));
     s.top_dz = dzs / src[6][1];                         // DZ=1.0E00/FLOAT(NPZ-1)/DZZDZ(2)
@@ -574,10 +614,18 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     s.plume = plume;
     std::free(hm);
 
-    // work decomposition: TX x TY tiles, z chunks of >= 3 planes
+    // work decomposition: TX x TY tiles, z chunks of <= MHD3D_ZCHUNK planes;
+    // small grids take shorter chunks (>= 4 planes) so that the launch still
+    // fills about two waves of the SMs
     h->ntx = (npx + TX - 1) / TX;
-    const int target = MHD3D_ZCHUNK;
-    int nch = (npz + target - 1) / target;
+    const int tyw = h->f32 ? TY32 : TY;
+    const long ntiles = (long)h->ntx * ((npy + tyw - 1) / tyw);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+    const long want = 2L * sms * (h->f32 ? 5 : 3);
+    int nch = (npz + MHD3D_ZCHUNK - 1) / MHD3D_ZCHUNK;
+    const int fill = (int)std::min<long>((want + ntiles - 1) / ntiles, npz / 4);
+    if (fill > nch) nch = fill;
     while (nch > 1 && npz / nch < 3) --nch;
     h->nchunks = nch;
     h->zlen = npz / nch;
@@ -628,6 +676,20 @@ int set_background(Handle* h)
         const int u = k + 1;   // U plane of interior plane k (Fortran K = k+2)
         const double az = h->faz_h[u], bzq = h->fbz_h[u], czq = h->fcz_h[u];
         PlaneBg& q = pb[k];
+        q.az = (float)az;
+        q.bzq = (float)bzq;
+        q.czq = (float)czq;
+        q.rka = (float)h->rka_h[u];
+        q.dka = (float)h->dka_h[u];
+        q.rddz = (float)(1.0 / h->ddz_h[u]);
+        q.ddz = (float)h->ddz_h[u];
+        q.fw2z = (float)(0.5 * h->p.repr * h->p.cv / h->rka_h[u]);
+        q.robm = (float)R[u - 1];
+        q.robc = (float)R[u];
+        q.robp = (float)R[u + 1];
+        q.ttbm = (float)T[u - 1];
+        q.ttbc = (float)T[u];
+        q.ttbp = (float)T[u + 1];
         const double tz = T[u + 1] - T[u - 1];
         q.tz = (float)tz;
         q.tlz = (float)(tz * bzq + (T[u + 1] + T[u - 1] - 2.0 * T[u]) * czq);

@@ -127,13 +127,34 @@ constexpr int BW32 = 36;                // TMA box row: x0-1 .. x0+34 (36 floats
 constexpr int BH32 = TY32 + 2;
 constexpr int BSLOT32 = BW32 * BH32;
 
-struct PlaneBg {
-    float tz;                 // Tb(K+1)-Tb(K-1)
-    float tlz;                // z part of the Laplacian of Tb: tz*BZQ(K) + (Tb(K+1)+Tb(K-1)-2Tb(K))*CZQ(K)
-    float fw;                 // GRAV*RHOb(K) - (Pb(K+1)-Pb(K-1))*AZ(K), Pb=RHOb*Tb
-    float bx, by, bz;         // Bb(K)
-    float bxz, byz, bzz;      // Bb(K+1)-Bb(K-1)
-    float bxlz, bylz, bzlz;   // z part of the Laplacian of Bb (one-sided on the walls, like B's)
+// Per-plane constants of the FP32 kernel, rounded once from FP64 on the host
+// and read as one aligned record per plane.
+struct alignas(16) PlaneBg {
+    float az, bzq, czq, rka, dka;   // HZ*DZZDZ, HZ*D2ZZDZ2, H2Z*DZZDZ**2, RKAPA, DKAPA
+    float rddz, ddz, fw2z;          // 1/DDZ, DDZ, 0.5*REPR*CV/RKAPA (CFL)
+    float robm, robc, robp;         // RHOb of planes K-1, K, K+1
+    float ttbm, ttbc, ttbp;         // Tb of planes K-1, K, K+1
+    float tz;                       // Tb(K+1)-Tb(K-1)
+    float tlz;                      // z part of the Laplacian of Tb: tz*BZQ(K) + (Tb(K+1)+Tb(K-1)-2Tb(K))*CZQ(K)
+    float fw;                       // GRAV*RHOb(K) - (Pb(K+1)-Pb(K-1))*AZ(K), Pb=RHOb*Tb
+    float bx, by, bz;               // Bb(K)
+    float bxz, byz, bzz;            // Bb(K+1)-Bb(K-1)
+    float bxlz, bylz, bzlz;         // z part of the Laplacian of Bb (one-sided on the walls, like B's)
+    float pad[2];
+};
+
+// Run constants of the FP32 kernel (Scalars rounded once to FP32).
+struct Scalars32 {
+    float grav, ore, c13, c43, tmp13, tmpa, tmpb, tmpc, ocv;
+    float omx, omz, orm, obeta, tmpm;
+    float ogamma, gamma, cw3;
+};
+
+// Per-column constants of the FP32 kernel: HX*DXXDX, HX*D2XXDX2,
+// H2X*DXXDX**2, 1/DDX, DDX (and the same in y).
+struct alignas(16) ColC {
+    float a, b, c, rdd;
+    float dd, pad[3];
 };
 
 struct StageArgs32 {
@@ -151,6 +172,9 @@ struct StageArgs32 {
     const float* ttb;         // Tb at every U plane
     const double* bgd;        // FP64 backgrounds: RHOb, Tb, BXb, BYb, BZb, NZ values each
     const PlaneBg* pb;        // per interior plane
+    const ColC* cx;           // per x column (Fortran I=1..NX)
+    const ColC* cy;           // per y row (Fortran J=1..NY)
+    Scalars32 s32;
     double top_lin, top_tb;   // C43*Tb(3)-C13*Tb(4)-Tb(2) and Tb(2): top-wall temperature in perturbation form
     float t_top_fix, t_top_fix4, t_top_flux, t_bot;   // wall T' constants (ITC 0/2/4, ITC=4 left half, ITC=1; IZC)
     size_t uf, uz, zf, zz;

@@ -9,8 +9,9 @@
 // background's difference, formed on the host in FP64 (PlaneBg), so no FP32
 // operation cancels two background-sized numbers.  The pressure enters as
 // P' = RHOb*T' + RO'*(Tb + T') and the gravity/pressure balance of the
-// background as one FP64-formed number per plane.  The CFL limits and the
-// Mach number are formed and reduced in FP64 from the FP32 state.
+// background as one FP64-formed number per plane.  The step's CFL limits and
+// Mach number are formed per cell in FP32 and reduced through FP64 keys; the
+// standalone CFL pass (first step, state changes) forms them in FP64.
 //
 // Work decomposition and plane ring as in the FP64 kernel: a CTA owns a
 // 32 x TY32 tile of columns and a chunk of z planes; planes arrive by TMA
@@ -76,8 +77,71 @@ __device__ __forceinline__ float qf(const float* __restrict__ raw, const float* 
     }
 }
 
+// Stage-3 CFL limits of the FP32 form: formed per cell in FP32 (the
+// contracted form of the FP64 FMA build: W1 = DD/(|u|+c_f), W2 and W3 from
+// Y=DD*DD*RO), reduced per warp in FP32 and across warps and CTAs as FP64
+// keys.  One FP64 reduction per step; DT carries FP32's relative precision.
+struct CflAcc32 {
+    float smax = 0.f;                          // max over cells of (|u|+c_f)/DD
+    float wmin = __builtin_huge_valf();        // min of W2, W3
+    float m2 = -__builtin_huge_valf();         // max of MACH**2
+    unsigned bad = 0;
+};
+
+template <bool MAG>
+__device__ __forceinline__ void cfl32_cell(CflAcc32& c, float ogamma, float gamma, float obeta, float cw3, float rdd,
+                                           float dd, float fw2, float ru, float rv, float rw, float ro, float tt,
+                                           float bx, float by, float bz)
+{
+    const float r = __frcp_rn(ro);
+    const float uu = (ru * ru + rv * rv + rw * rw) * (r * r);
+    const float mach2 = ogamma * uu * __frcp_rn(tt);
+    float a2 = gamma * tt;
+    if (MAG) a2 += (bx * bx + by * by + bz * bz) * obeta * r;
+    const float sp = sqrtf(uu) + sqrtf(a2);
+    const float sr = sp * rdd;
+    const float y = dd * dd * ro;
+    const float w = fminf(cw3 * y, fw2 * y);
+    c.smax = fmaxf(c.smax, sr);
+    c.wmin = fminf(c.wmin, w);
+    c.m2 = fmaxf(c.m2, mach2);
+    c.bad |= (unsigned)(!(sr > 0.f && sr <= FLT_MAX) || !(fabsf(w) <= FLT_MAX) || !(fabsf(mach2) <= FLT_MAX));
+}
+
+__device__ __forceinline__ void cfl32_commit(Accum* acc, unsigned long long* red, const CflAcc32& c)
+{
+    float smax = c.smax, wmin = c.wmin, m2 = c.m2;
+    unsigned bad = c.bad;
+    for (int o = 16; o > 0; o >>= 1) {
+        smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        wmin = fminf(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+        m2 = fmaxf(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    unsigned long long* r = red + (threadIdx.x >> 5) * 3;
+    if ((threadIdx.x & 31) == 0) {
+        double w = (double)wmin;
+        if (smax > 0.f) w = fmin(w, 1.0 / (double)smax);
+        r[0] = key_of(w);
+        r[1] = key_of((double)m2);
+        r[2] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long kmin = ~0ull, kmu = 0ull, b = 0ull;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            kmin = min(kmin, red[i * 3 + 0]);
+            kmu = max(kmu, red[i * 3 + 1]);
+            b |= red[i * 3 + 2];
+        }
+        atomicMin(&acc->wmin[0], kmin);
+        atomicMax(&acc->umax, kmu);
+        if (b) atomicOr(&acc->bad, 1u);
+    }
+}
+
 #ifndef MHD3D_MINB32
-#define MHD3D_MINB32 4
+#define MHD3D_MINB32 5   // 5 x 128 threads x 96 registers, 5 x 34 KB shared
 #endif
 
 template <bool MAG, bool ROT, int STAGE>
@@ -114,16 +178,15 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
     const double DT = ctl->dt;
     const float cu = (float)(STAGE == 1 ? s.gam1 * DT : STAGE == 2 ? s.gam2 * DT : s.gam3 * DT);
     const float cz = (float)(STAGE == 1 ? s.zeta1 * DT : s.zeta2 * DT);
-    const float C13 = (float)s.c13, C43 = (float)s.c43;
+    const Scalars32& f = a.s32;
+    const float C13 = f.c13, C43 = f.c43;
 
-    const float ax = active ? (float)m.fax[gi + 1] : 0.f, bxq = active ? (float)m.fbx[gi + 1] : 0.f;
-    const float cxq = active ? (float)m.fcx[gi + 1] : 0.f;
-    const float ay = active ? (float)m.fay[gj + 1] : 0.f, byq = active ? (float)m.fby[gj + 1] : 0.f;
-    const float cyq = active ? (float)m.fcy[gj + 1] : 0.f;
-    const float grav = (float)s.grav, ore = (float)s.ore, c43 = (float)s.c43, tmp13 = (float)s.tmp_13;
-    const float tmpa = (float)s.tmp_a, tmpb = (float)s.tmp_b, tmpc = (float)s.tmp_cond, ocv = (float)s.ocv;
-    const float omx = (float)s.omx, omz = (float)s.omz, orm = (float)s.orm, obeta = (float)s.obeta;
-    const float tmpm = (float)s.tmp_m;
+    const ColC cxc = a.cx[active ? gi + 1 : 0], cyc = a.cy[active ? gj + 1 : 0];
+    const float ax = cxc.a, bxq = cxc.b, cxq = cxc.c;
+    const float ay = cyc.a, byq = cyc.b, cyq = cyc.c;
+    // stage-3 CFL: per-column 1/DD and DD parts
+    const float rddxy = fmaxf(cxc.rdd, cyc.rdd);
+    const float ddxy = fminf(cxc.dd, cyc.dd);
 
     const unsigned raw_bytes = (unsigned)(NF * BSLOT32 * 4);
     const unsigned z_bytes = (unsigned)(NF * TY32 * TX * 4);
@@ -176,7 +239,11 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
     }
     bool zpending = false;
     int zfill = 0;
-    CflAcc cfa;
+    CflAcc32 cfa;
+    auto cfl_at = [&](const PlaneBg& q, float ru, float rv, float rw, float ro, float tt, float bx, float by, float bz) {
+        cfl32_cell<MAG>(cfa, f.ogamma, f.gamma, f.obeta, f.cw3, fmaxf(rddxy, q.rddz), fminf(ddxy, q.ddz), q.fw2z, ru,
+                        rv, rw, ro, tt, bx, by, bz);
+    };
 
     for (int k = k0; k < k1; ++k) {
         if (STAGE >= 2 && tid == 0 && !*sflag) {
@@ -197,15 +264,14 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
             const float* Im = sri + (size_t)((k + 0) % 3) * BSLOT32;
             const float* Ic = sri + (size_t)((k + 1) % 3) * BSLOT32;
             const float* Ip = sri + (size_t)((k + 2) % 3) * BSLOT32;
-            const float robm = a.rob[k], robc = a.rob[k + 1], robp = a.rob[k + 2];
-            const float ttbm = a.ttb[k], ttbc = a.ttb[k + 1], ttbp = a.ttb[k + 2];
+            const PlaneBg& pb = a.pb[k];
+            const float robm = pb.robm, robc = pb.robc, robp = pb.robp;
+            const float ttbm = pb.ttbm, ttbc = pb.ttbc, ttbp = pb.ttbp;
 #define C_(q, dx, dy) qf<q>(Rc, Ic, (ly + (dy)) * BW32 + (lx + (dx)), robc, ttbc)
 #define M_(q, dx, dy) qf<q>(Rm, Im, (ly + (dy)) * BW32 + (lx + (dx)), robm, ttbm)
 #define P_(q, dx, dy) qf<q>(Rp, Ip, (ly + (dy)) * BW32 + (lx + (dx)), robp, ttbp)
-            const PlaneBg pb = a.pb[k];
             const bool top = (k == 0), bot = (k == npz - 1);
-            const float az = (float)m.faz[k + 1], bzq = (float)m.fbz[k + 1], czq = (float)m.fcz[k + 1];
-            const float rka = (float)m.rkapa[k + 1], dka = (float)m.dkapa[k + 1];
+            const float az = pb.az, bzq = pb.bzq, czq = pb.czq, rka = pb.rka, dka = pb.dka;
             // own column two and three planes inside the wall (one-sided stencils)
             float rw2 = 0.f, ww2 = 0.f, bx2 = 0.f, bx3 = 0.f, by2 = 0.f, by3 = 0.f;
             if (top || bot) {
@@ -248,7 +314,7 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                          + (C_(P_RV, 1, 0) * u_xp - C_(P_RV, -1, 0) * u_xm) * ax
                          + (C_(P_RV, 0, 1) * v_yp - C_(P_RV, 0, -1) * v_ym) * ay
                          + (P_(P_RV, 0, 0) * w_zp - M_(P_RV, 0, 0) * w_zm) * az);
-            float fw = grav * ROp + pb.fw
+            float fw = f.grav * ROp + pb.fw
                      - ((P_(P_PP, 0, 0) - M_(P_PP, 0, 0)) * az
                         + (C_(P_RW, 1, 0) * u_xp - C_(P_RW, -1, 0) * u_xm) * ax
                         + (C_(P_RW, 0, 1) * v_yp - C_(P_RW, 0, -1) * v_ym) * ay
@@ -263,7 +329,7 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                 const float dtz = dtzp + pb.tz;
                 const float lap = dtx * bxq + (txp + txm - 2.f * TTp) * cxq + dty * byq + (typ + tym - 2.f * TTp) * cyq
                                 + dtzp * bzq + (tzp + tzm - 2.f * TTp) * czq + pb.tlz;
-                ft = -(uc * dtx * ax + vc * dty * ay + wc * dtz * az) + RIc * tmpc * (rka * lap + dka * dtz * az);
+                ft = -(uc * dtx * ax + vc * dty * ay + wc * dtz * az) + RIc * f.tmpc * (rka * lap + dka * dtz * az);
             }
             // viscous stress
             {
@@ -276,9 +342,9 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                 const float lxw = (w_xp - w_xm) * bxq + (w_xp + w_xm - 2.f * wc) * cxq;
                 const float lyw = (w_yp - w_ym) * byq + (w_yp + w_ym - 2.f * wc) * cyq;
                 const float lzw = (w_zp - w_zm) * bzq + (w_zp + w_zm - 2.f * wc) * czq;
-                fu += ore * (c43 * lxu + lyu + lzu);
-                fv += ore * (lxv + c43 * lyv + lzv);
-                fw += ore * (lxw + lyw + c43 * lzw);
+                fu += f.ore * (f.c43 * lxu + lyu + lzu);
+                fv += f.ore * (lxv + f.c43 * lyv + lzv);
+                fw += f.ore * (lxw + lyw + f.c43 * lzw);
             }
             // velocity gradients, the 19-point cross terms, heating
             const float ux = (u_xp - u_xm) * ax, vx = (v_xp - v_xm) * ax, wx = (w_xp - w_xm) * ax;
@@ -292,18 +358,18 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                 const float dywz = ((P_(P_WW, 0, 1) - M_(P_WW, 0, 1)) - (P_(P_WW, 0, -1) - M_(P_WW, 0, -1))) * ayz;
                 const float dxuz = ((P_(P_UU, 1, 0) - M_(P_UU, 1, 0)) - (P_(P_UU, -1, 0) - M_(P_UU, -1, 0))) * axz;
                 const float dyvz = ((P_(P_VV, 0, 1) - M_(P_VV, 0, 1)) - (P_(P_VV, 0, -1) - M_(P_VV, 0, -1))) * ayz;
-                fu += tmp13 * (dyvx + dxwz);
-                fv += tmp13 * (dyux + dywz);
-                fw += tmp13 * (dxuz + dyvz);
+                fu += f.tmp13 * (dyvx + dxwz);
+                fv += f.tmp13 * (dyux + dywz);
+                fw += f.tmp13 * (dxuz + dyvz);
             }
-            float heat = tmpa * (c43 * ux * ux + vx * vx + wx * wx + uy * uy + 2.f * uy * vx + uz * uz + vz * vz
+            float heat = f.tmpa * (f.c43 * ux * ux + vx * vx + wx * wx + uy * uy + 2.f * uy * vx + uz * uz + vz * vz
                                  + wy * wy + 2.f * vz * wy + 2.f * uz * wx)
-                       + tmpb * (vy * vy + wz * wz - ux * wz - ux * vy - vy * wz);
-            ft -= ocv * (ttbc + TTp) * (ux + vy + wz);
+                       + f.tmpb * (vy * vy + wz * wz - ux * wz - ux * vy - vy * wz);
+            ft -= f.ocv * (ttbc + TTp) * (ux + vy + wz);
             if (ROT) {
-                fu += omz * RVc;
-                fv += omx * RWc - omz * RUc;
-                fw -= omx * RVc;
+                fu += f.omz * RVc;
+                fv += f.omx * RWc - f.omz * RUc;
+                fw -= f.omx * RVc;
             }
             // induction, Lorentz force, Ohmic heating
             float w1 = 0.f, w2 = 0.f, w3 = 0.f;
@@ -339,14 +405,14 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                 const float lbz = (bzxp - bzxm) * bxq + (bzxp + bzxm - 2.f * BZp) * cxq
                                 + (bzyp - bzym) * byq + (bzyp + bzym - 2.f * BZp) * cyq
                                 + (bzzp - bzzm) * bzq + (bzzp + bzzm - 2.f * BZp) * czq + pb.bzlz;
-                w1 = BYc * uy - BXc * vy + BZc * uz - BXc * wzm - (uc * bxx + vc * bxy + wc * bxz) + orm * lbx;
-                w2 = BXc * vx - BYc * ux + BZc * vz - BYc * wzm - (uc * byx + vc * byy + wc * byz) + orm * lby;
-                w3 = BXc * wx - BZc * ux + BYc * wy - BZc * vy - (uc * bzx + vc * bzy + wc * bzz) + orm * lbz;
+                w1 = BYc * uy - BXc * vy + BZc * uz - BXc * wzm - (uc * bxx + vc * bxy + wc * bxz) + f.orm * lbx;
+                w2 = BXc * vx - BYc * ux + BZc * vz - BYc * wzm - (uc * byx + vc * byy + wc * byz) + f.orm * lby;
+                w3 = BXc * wx - BZc * ux + BYc * wy - BZc * vy - (uc * bzx + vc * bzy + wc * bzz) + f.orm * lbz;
                 const float jz = bxy - byx, jy = bxz - bzx, jx = byz - bzy;
-                fu += obeta * (BYc * jz + BZc * jy);
-                fv += obeta * (BZc * jx - BXc * jz);
-                fw -= obeta * (BXc * jy + BYc * jx);
-                heat += tmpm * (jx * jx + jy * jy + jz * jz);
+                fu += f.obeta * (BYc * jz + BZc * jy);
+                fv += f.obeta * (BZc * jx - BXc * jz);
+                fw -= f.obeta * (BXc * jy + BYc * jx);
+                heat += f.tmpm * (jx * jx + jy * jy + jz * jz);
             }
             ft += RIc * heat;
             // ghost RO planes: FLUXES leaves 1/RO behind (3dmhdsub.f:1386-1391)
@@ -419,13 +485,9 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                         }
                     }
                 }
-                const double* bgd = a.bgd;
-                const size_t NZ = (size_t)npz + 2;
-                auto full = [&](int which, int kp, float v) -> double { return bgd[which * NZ + kp + 1] + (double)v; };
                 if (!top && !bot && STAGE == 3)
-                    cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, (double)nu, (double)nv, (double)nw, full(0, k, nr),
-                                      full(1, k, nt), MAG ? full(2, k, nbx) : 0.0, MAG ? full(3, k, nby) : 0.0,
-                                      MAG ? full(4, k, nbz) : 0.0);
+                    cfl_at(pb, nu, nv, nw, robc + nr, ttbc + nt, MAG ? pb.bx + nbx : 0.f, MAG ? pb.by + nby : 0.f,
+                           MAG ? pb.bz + nbz : 0.f);
                 if (k == 2 && k0 == 0) {
                     // top wall (plane 0) from planes 1 (read back) and 2 (this plane)
                     const float* ub = a.u_out + ucol;
@@ -461,10 +523,11 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                         else
                             store_cell<4, float>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.f, tt_w});
                     }
-                    if (STAGE == 3)
-                        cfl_acc_direct<MAG>(cfa, s, m, gi, gj, 0, (double)ru_w, (double)rv_w, 0.0, full(0, 0, w0_rop),
-                                            full(1, 0, tt_w), MAG ? full(2, 0, w0_bx) : 0.0,
-                                            MAG ? full(3, 0, w0_by) : 0.0, MAG ? full(4, 0, bz_w) : 0.0);
+                    if (STAGE == 3) {
+                        const PlaneBg& p0 = a.pb[0];
+                        cfl_at(p0, ru_w, rv_w, 0.f, w0_ro, p0.ttbc + tt_w, MAG ? p0.bx + w0_bx : 0.f,
+                               MAG ? p0.by + w0_by : 0.f, MAG ? p0.bz + bz_w : 0.f);
+                    }
                 }
                 if (bot) {
                     // bottom wall (this plane) from planes npz-2 and npz-3, read back
@@ -488,9 +551,8 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
                             store_cell<4, float>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.f, tt_w});
                     }
                     if (STAGE == 3)
-                        cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, (double)ru_w, (double)rv_w, 0.0, full(0, k, nr),
-                                          full(1, k, tt_w), MAG ? full(2, k, nbx) : 0.0, MAG ? full(3, k, nby) : 0.0,
-                                          MAG ? full(4, k, bz_w) : 0.0);
+                        cfl_at(pb, ru_w, rv_w, 0.f, nrf, ttbc + tt_w, MAG ? pb.bx + nbx : 0.f, MAG ? pb.by + nby : 0.f,
+                               MAG ? pb.bz + bz_w : 0.f);
                 }
             }
         } else if (STAGE >= 2) {
@@ -515,7 +577,7 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
         }
         return;
     }
-    if (STAGE == 3) cfl_commit_acc(a.acc, red, cfa);
+    if (STAGE == 3) cfl32_commit(a.acc, red, cfa);
 }
 
 // CFL reduction over the current FP32 state, formed in FP64 (first step,
