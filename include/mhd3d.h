@@ -174,6 +174,26 @@ int mhd3d_cfl(void* handle, double* dt, double* umach);
 int mhd3d_bcon(void* handle);
 
 /*
+ * Horizontally averaged profiles of the current state: the averages the
+ * reference forms with HORIZONTAL_MEAN (3dmhdsub.f:3143-3223: the sum over
+ * the interior I=2..NX-1, J=2..NY-1 divided by FLOAT(NPX*NPY)) for its flux
+ * diagnostics (3dmhdsub.f:1519-1528, 1651-1676), computed on the device in
+ * FP64.  out holds MHD3D_NPROF rows of NPZ values, row r at
+ * out[r*NPZ + (K-2)] for the interior planes K=2..NZ-1.  With u=RU/RO etc.:
+ */
+#define MHD3D_NPROF        7
+#define MHD3D_PROF_RHO     0  /* <RO>                                                  */
+#define MHD3D_PROF_T       1  /* <TT>, TTM (1523)                                      */
+#define MHD3D_PROF_KE      2  /* <0.5*RO*|u|**2>                                       */
+#define MHD3D_PROF_ENTH    3  /* <2.5*RO*TT>, c_p=2.5 as the reference takes it (1654) */
+#define MHD3D_PROF_FCONV   4  /* <-RW*(2.5*(TT-TTM)+0.5*|u|**2)>, FCONM (1653-1661)    */
+#define MHD3D_PROF_FRAD    5  /* (TTM(K+1)-TTM(K-1))*HZ*DZZDZ*RKAPA/REPR, one-sided at
+                                 K=2 and K=NZ-1, FRADM (1663-1676)                    */
+#define MHD3D_PROF_ME      6  /* <0.5*|B|**2> (0 without LMAG; no counterpart in the
+                                 reference)                                           */
+int mhd3d_profiles(void* handle, double* out);
+
+/*
  * Stream control and asynchronous stepping (no counterpart in the
  * reference; they let a host overlap its own work with the step, capture
  * steps in a CUDA graph and time them on its own stream).

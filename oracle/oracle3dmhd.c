@@ -1022,3 +1022,54 @@ void oracle_fluxes(oracle3dmhd* o, double* fu, double* fv, double* fw, double* f
     }
     for (int a = 0; a < 8; ++a) { memcpy(cur[a], save[a], nb); free(save[a]); }
 }
+
+/* HORIZONTAL_MEAN (3dmhdsub.f:3143-3223, NGRID=0 branch): the sum over
+ * I=IX/2+1..NX-IX/2, J=IY/2+1..NY-IY/2 of plane K, J outer, divided by
+ * FLOAT(NPX*NPY).  The per-cell quantities are those of the flux diagnostics
+ * (1651-1661) with u=RU*(1/RO) as FLUXES forms it (1386-1425). */
+void oracle_profiles(const oracle3dmhd* o, double* out)
+{
+    const int npz = o->p.npz;
+    const double cnt = (double)(float)(o->p.npx * o->p.npy);
+    double* ttm = (double*)malloc(sizeof(double) * (size_t)NZ);
+    for (int k = 2; k <= NZ - 1; ++k) {
+        double sro = 0.0, stt = 0.0, ske = 0.0, sen = 0.0, sme = 0.0;
+        for (int j = 2; j <= NY - 1; ++j)
+            for (int i = 2; i <= NX - 1; ++i) {
+                const size_t c = IDX(i, j, k);
+                const double ro = o->ro[c], tt = o->tt[c];
+                const double ri = 1.0 / ro;
+                const double u = o->ru[c] * ri, v = o->rv[c] * ri, w = o->rw[c] * ri;
+                sro = sro + ro;
+                stt = stt + tt;
+                ske = ske + 0.5 * ro * (u * u + v * v + w * w);
+                sen = sen + 2.5 * ro * tt;
+                if (o->p.lmag) sme = sme + 0.5 * (o->bx[c] * o->bx[c] + o->by[c] * o->by[c] + o->bz[c] * o->bz[c]);
+            }
+        const int r = k - 2;
+        out[MHD3D_PROF_RHO * npz + r] = sro / cnt;
+        out[MHD3D_PROF_T * npz + r] = ttm[k - 1] = stt / cnt;
+        out[MHD3D_PROF_KE * npz + r] = ske / cnt;
+        out[MHD3D_PROF_ENTH * npz + r] = sen / cnt;
+        out[MHD3D_PROF_ME * npz + r] = sme / cnt;
+        /* FCONM: WW2=-RW*(2.5*WW1+0.5*(UU*UU+VV*VV+WW*WW)), WW1=TT-TTM (1524-1528, 1653-1656) */
+        double sfc = 0.0;
+        for (int j = 2; j <= NY - 1; ++j)
+            for (int i = 2; i <= NX - 1; ++i) {
+                const size_t c = IDX(i, j, k);
+                const double ri = 1.0 / o->ro[c];
+                const double u = o->ru[c] * ri, v = o->rv[c] * ri, w = o->rw[c] * ri;
+                sfc = sfc + -o->rw[c] * (2.5 * (o->tt[c] - ttm[k - 1]) + 0.5 * (u * u + v * v + w * w));
+            }
+        out[MHD3D_PROF_FCONV * npz + r] = sfc / cnt;
+    }
+    /* FRADM (1663-1676) */
+    for (int k = 2; k <= NZ - 1; ++k) {
+        double d;
+        if (k == 2) d = -3.0 * ttm[1] + 4.0 * ttm[2] - ttm[3];
+        else if (k == NZ - 1) d = 3.0 * ttm[NZ - 2] - 4.0 * ttm[NZ - 3] + ttm[NZ - 4];
+        else d = ttm[k] - ttm[k - 2];
+        out[MHD3D_PROF_FRAD * npz + (k - 2)] = d * o->p.hz * o->dzzdz[k] * o->rkapa[k] / o->p.repr;   /* 1-based */
+    }
+    free(ttm);
+}

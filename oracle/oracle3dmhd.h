@@ -60,6 +60,12 @@ int oracle_cfl(oracle3dmhd* o, double* dt, double* umach);
 /* BCON (3dmhdsub.f:2639-2958) in place. */
 void oracle_bcon(oracle3dmhd* o);
 
+/* Horizontally averaged profiles (HORIZONTAL_MEAN, 3dmhdsub.f:3143-3223) of
+ * the current state in the rows of mhd3d_profiles (include/mhd3d.h):
+ * out[r*NPZ + (K-2)], K=2..NZ-1.  Sums run in the reference's order (J outer,
+ * I inner) and are divided by FLOAT(NPX*NPY). */
+void oracle_profiles(const oracle3dmhd* o, double* out);
+
 /* OpenMP threads used by the sweeps (<=0: leave the runtime default). */
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

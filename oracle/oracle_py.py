@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_EXE = os.path.join(HERE, "_ref", "ref3dmhd")
 
 FIELDS = ("ru", "rv", "rw", "tt", "ro", "bx", "by", "bz")
+NPROF = 7   # MHD3D_NPROF rows: rho, T, KE, enthalpy, convective flux, radiative flux, magnetic energy
 FLUXES = ("fu", "fv", "fw", "fr", "ft", "ww1", "ww2", "ww3")
 GRID_NAMES = ("exx", "dxxdx", "d2xxdx2", "ddx", "wyy", "dyydy", "d2yydy2", "ddy",
               "zee", "dzzdz", "d2zzdz2", "ddz", "rkapa", "dkapa")
@@ -50,6 +51,7 @@ def oracle_lib():
         lib.oracle_fluxes.argtypes = [vp] + [vp] * 8
         lib.oracle_cfl.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.oracle_bcon.argtypes = [vp]
+        lib.oracle_profiles.argtypes = [vp, vp]
         lib.oracle_set_threads.argtypes = [C.c_int]
         lib.oracle_get_threads.restype = C.c_int
         _lib = lib
@@ -110,6 +112,12 @@ class Oracle:
     def bcon(self):
         self.lib.oracle_bcon(self.h)
 
+    def profiles(self) -> np.ndarray:
+        """Horizontal-mean profiles, rows MHD3D_PROF_* x interior planes."""
+        out = np.zeros((NPROF, self.params.npz))
+        self.lib.oracle_profiles(self.h, _ptr(out))
+        return out
+
 
 def set_threads(n: int):
     oracle_lib().oracle_set_threads(n)
@@ -125,6 +133,8 @@ def run_reference(params, grid: dict, state: dict, nsteps: int, npey: int = 1, n
 
     mode 0: nsteps x STEP, returns the fields and DT/TIMC/TIMT/UMACH/NIT.
     mode 1: one FLUXES, returns the right-hand sides.
+    mode 2: the MHD3D_PROF_* profiles averaged by the reference's
+            HORIZONTAL_MEAN, returned as {"profiles": (NPROF, NPZ) array}.
     warmup steps run before the timed ones ("seconds" covers the nsteps only).
     """
     nfld = 8 if params.lmag else 5
@@ -142,6 +152,10 @@ def run_reference(params, grid: dict, state: dict, nsteps: int, npey: int = 1, n
         if r.returncode != 0:
             raise RuntimeError(f"reference run failed ({r.returncode}): {r.stderr[-2000:]}")
         data = open(fout, "rb").read()
+    if mode == 2:
+        assert data[:4] == b"R3DP"
+        return {"profiles": np.frombuffer(data, dtype=np.float64, count=NPROF * params.npz, offset=4)
+                .reshape(NPROF, params.npz).copy()}
     assert data[:4] == b"R3DO"
     st, nit = struct.unpack_from("<2i", data, 4)
     dt, timc, timt, umach, nitd, secs = struct.unpack_from("<6d", data, 12)

@@ -11,7 +11,10 @@
  * slab the reference's decomposition assigns it (3dmhd.f:87-88,
  * 3dmhdparam.f:17-19), sets the COMMON blocks the way the main program does
  * (3dmhd.f:105-240), runs CALL STEP nsteps times (mode 0) or CALL FLUXES
- * once (mode 1), and gathers the result into OUT.
+ * once (mode 1), and gathers the result into OUT.  Mode 2 averages the
+ * diagnostic quantities of include/mhd3d.h (MHD3D_PROF_*) with the
+ * reference's own HORIZONTAL_MEAN (3dmhdsub.f:3143-3223) on every rank and
+ * writes the MHD3D_NPROF x NPZ profile rows instead of fields.
  *
  * MPI is emulated: SEND/RECV/SENDRECV over socket pairs between the ranks
  * that talk to each other in COMM_MPI, ALLREDUCE/BCAST through shared
@@ -340,6 +343,40 @@ int main(int argc, char** argv)
                     memcpy(loc[a] + (size_t)NX * (j + (size_t)NY * k),
                            fin[a] + (size_t)NXg * ((j + joff) + (size_t)NYg * (k + koff)), sizeof(double) * NX);
         }
+        if (mode == 2) {
+            /* per-cell quantities of the flux diagnostics (1651-1661) on the
+               local array, averaged by HORIZONTAL_MEAN; WW1=TT-TTM (1524-1528) */
+            const size_t nl = (size_t)NX * NY * NZ;
+            const double *ru = loc[0], *rv = loc[1], *rw = loc[2], *tt = loc[3], *ro = loc[4];
+            double* q = (double*)calloc(nl, sizeof(double));
+            double* m = (double*)calloc((size_t)NZ * MHD3D_NPROF, sizeof(double));
+            sub_HORIZONTAL_MEAN(m + MHD3D_PROF_RHO * NZ, ro);
+            sub_HORIZONTAL_MEAN(m + MHD3D_PROF_T * NZ, tt);
+            const double* ttm = m + MHD3D_PROF_T * NZ;
+            for (int pass = 0; pass < 4; ++pass) {
+                for (int k = 1; k <= NZ; ++k)
+                    for (int j = 1; j <= NY; ++j)
+                        for (int i = 1; i <= NX; ++i) {
+                            const size_t c = (size_t)(i - 1) + (size_t)NX * ((size_t)(j - 1) + (size_t)NY * (k - 1));
+                            const double ri = 1.0 / ro[c];
+                            const double u = ru[c] * ri, v = rv[c] * ri, w = rw[c] * ri;
+                            if (pass == 0) q[c] = 0.5 * ro[c] * (u * u + v * v + w * w);
+                            else if (pass == 1) q[c] = 2.5 * ro[c] * tt[c];
+                            else if (pass == 2) q[c] = -rw[c] * (2.5 * (tt[c] - ttm[k - 1]) + 0.5 * (u * u + v * v + w * w));
+                            else q[c] = P.lmag ? 0.5 * (loc[5][c] * loc[5][c] + loc[6][c] * loc[6][c] + loc[7][c] * loc[7][c]) : 0.0;
+                        }
+                const int row = pass == 0 ? MHD3D_PROF_KE : pass == 1 ? MHD3D_PROF_ENTH : pass == 2 ? MHD3D_PROF_FCONV : MHD3D_PROF_ME;
+                sub_HORIZONTAL_MEAN(m + row * NZ, q);
+            }
+            if (mypey == 0)
+                for (int r2 = 0; r2 < MHD3D_NPROF; ++r2)
+                    for (int k = 2; k <= NZ - 1; ++k)
+                        gout[(size_t)r2 * P.npz + (size_t)(k - 2 + koff)] = m[(size_t)r2 * NZ + (k - 1)];
+            free(q);
+            free(m);
+            barrier();
+            _exit(0);
+        }
         if (mode == 0)
             for (int s = 0; s < warmup; ++s) sub_STEP();
         barrier();
@@ -383,6 +420,25 @@ int main(int argc, char** argv)
         if (wait(&st) < 0 || !WIFEXITED(st) || WEXITSTATUS(st) != 0) failed = 1;
     }
     if (failed) { fprintf(stderr, "ref3dmhd: a rank failed\n"); return 3; }
+    if (mode == 2) {
+        /* FRADM from the gathered TTM (3dmhdsub.f:1663-1676) */
+        const int npz = P.npz;
+        const double* ttm = gout + (size_t)MHD3D_PROF_T * npz;
+        for (int k = 0; k < npz; ++k) {
+            const int K = k + 2;
+            double d;
+            if (k == 0) d = -3.0 * ttm[0] + 4.0 * ttm[1] - ttm[2];
+            else if (k == npz - 1) d = 3.0 * ttm[npz - 1] - 4.0 * ttm[npz - 2] + ttm[npz - 3];
+            else d = ttm[k + 1] - ttm[k - 1];
+            gout[(size_t)MHD3D_PROF_FRAD * npz + k] = d * P.hz * met[9][K - 1] * met[12][K - 1] / P.repr;
+        }
+        FILE* o = fopen(argv[2], "wb");
+        if (!o) { perror(argv[2]); return 2; }
+        fwrite("R3DP", 1, 4, o);
+        fwrite(gout, sizeof(double), (size_t)MHD3D_NPROF * npz, o);
+        fclose(o);
+        return 0;
+    }
     /* periodic y halo rows as COMMUNICATE leaves them (x halos came with the rows) */
     for (int a = 0; a < nfld; ++a) {
         double* v = gout + (size_t)a * ng;

@@ -78,5 +78,6 @@ void sub_STEP(void);
 void sub_FLUXES(void);
 void sub_BCON(void);
 void sub_COMMUNICATE(void);
+void sub_HORIZONTAL_MEAN(double* VARM, double* VAR);
 
 #endif

@@ -184,6 +184,100 @@ __global__ void k_pack_interior32(const float* __restrict__ f, double* __restric
     }
 }
 
+// ---- horizontally averaged profiles (HORIZONTAL_MEAN, 3dmhdsub.f:3143-3223) ----
+// One block per interior plane; per-thread partial sums in a fixed order, then a
+// fixed tree, so the result is deterministic.  Per-cell formulas follow the
+// reference's flux diagnostics (1651-1661).
+constexpr int PROF_THREADS = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = PROF_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(PROF_THREADS) k_profiles(const void* __restrict__ ubuf, const double* __restrict__ bgd,
+                                                           double* __restrict__ out, int npx, int npy, int npz,
+                                                           int upitch, size_t uz, size_t uf, int lmag)
+{
+    __shared__ double red[PROF_THREADS];
+    const int k = blockIdx.x;   // interior plane, Fortran K = k+2
+    const int K0 = k + 1;       // U plane index
+    const size_t NZ = (size_t)npz + 2;
+    auto val = [&](int f, size_t off) -> double {
+        if (F32) {
+            const double v = (double)reinterpret_cast<const float*>(ubuf)[(size_t)f * uf + off];
+            const int bi = f == F_RO ? 0 : f == F_TT ? 1 : f == F_BX ? 2 : f == F_BY ? 3 : f == F_BZ ? 4 : -1;
+            return bi >= 0 ? bgd[bi * NZ + K0] + v : v;
+        }
+        return reinterpret_cast<const double*>(ubuf)[(size_t)f * uf + off];
+    };
+    const int n = npx * npy;
+    double sro = 0.0, stt = 0.0, ske = 0.0, sen = 0.0, sme = 0.0;
+    for (int q = threadIdx.x; q < n; q += PROF_THREADS) {
+        const int i = q % npx, j = q / npx;
+        const size_t off = (size_t)K0 * uz + (size_t)(j + 1) * upitch + (i + 1);
+        const double ro = val(F_RO, off), tt = val(F_TT, off);
+        const double ri = 1.0 / ro;
+        const double u = val(F_RU, off) * ri, v = val(F_RV, off) * ri, w = val(F_RW, off) * ri;
+        sro += ro;
+        stt += tt;
+        ske += 0.5 * ro * (u * u + v * v + w * w);
+        sen += 2.5 * ro * tt;
+        if (lmag) {
+            const double bx = val(F_BX, off), by = val(F_BY, off), bz = val(F_BZ, off);
+            sme += 0.5 * (bx * bx + by * by + bz * bz);
+        }
+    }
+    const double cnt = (double)(float)n;   // FLOAT(NPX*NPY)
+    const double rom = block_sum(sro, red) / cnt;
+    const double ttm = block_sum(stt, red) / cnt;
+    const double kem = block_sum(ske, red) / cnt;
+    const double enm = block_sum(sen, red) / cnt;
+    const double mem = block_sum(sme, red) / cnt;
+    double sfc = 0.0;
+    for (int q = threadIdx.x; q < n; q += PROF_THREADS) {
+        const int i = q % npx, j = q / npx;
+        const size_t off = (size_t)K0 * uz + (size_t)(j + 1) * upitch + (i + 1);
+        const double ro = val(F_RO, off), tt = val(F_TT, off), rw = val(F_RW, off);
+        const double ri = 1.0 / ro;
+        const double u = val(F_RU, off) * ri, v = val(F_RV, off) * ri, w = rw * ri;
+        sfc += -rw * (2.5 * (tt - ttm) + 0.5 * (u * u + v * v + w * w));
+    }
+    const double fcm = block_sum(sfc, red) / cnt;
+    if (threadIdx.x == 0) {
+        out[MHD3D_PROF_RHO * npz + k] = rom;
+        out[MHD3D_PROF_T * npz + k] = ttm;
+        out[MHD3D_PROF_KE * npz + k] = kem;
+        out[MHD3D_PROF_ENTH * npz + k] = enm;
+        out[MHD3D_PROF_FCONV * npz + k] = fcm;
+        out[MHD3D_PROF_ME * npz + k] = mem;
+    }
+}
+
+// FRADM from TTM (3dmhdsub.f:1663-1676): centred inside, one-sided at both walls
+__global__ void k_frad(double* __restrict__ out, const double* __restrict__ dzzdz, const double* __restrict__ rkapa,
+                       double hz, double repr, int npz)
+{
+    const double* ttm = out + MHD3D_PROF_T * npz;   // ttm[k] is TTM(K=k+2)
+    for (int k = threadIdx.x; k < npz; k += blockDim.x) {
+        const int K = k + 2;
+        double d;
+        if (k == 0) d = -3.0 * ttm[0] + 4.0 * ttm[1] - ttm[2];
+        else if (k == npz - 1) d = 3.0 * ttm[npz - 1] - 4.0 * ttm[npz - 2] + ttm[npz - 3];
+        else d = ttm[k + 1] - ttm[k - 1];
+        out[MHD3D_PROF_FRAD * npz + k] = d * hz * dzzdz[K - 1] * rkapa[K - 1] / repr;
+    }
+}
+
 __global__ void k_reset(Control* ctl, Accum* acc, int clear_stop, unsigned long long w4key)
 {
     for (int i = 0; i < 3; ++i) acc->wmin[i] = ~0ull;
@@ -916,6 +1010,27 @@ int fluxes(Handle* h, double* const out[8])
     return MHD3D_OK;
 }
 
+int profiles(Handle* h, double* out)
+{
+    CK(cudaSetDevice(h->dev));
+    if (!out) return MHD3D_ERR_ARG;
+    if (int st = settle(h)) return st;
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    double* dout = h->stage;   // the staging field holds far more than MHD3D_NPROF x NPZ doubles
+    if (h->f32)
+        k_profiles<true><<<npz, PROF_THREADS, 0, h->st>>>(h->ubuf[h->cur], h->bgd, dout, npx, npy, npz, h->upitch,
+                                                         h->uz, h->uf, h->p.lmag);
+    else
+        k_profiles<false><<<npz, PROF_THREADS, 0, h->st>>>(h->ubuf[h->cur], h->bgd, dout, npx, npy, npz, h->upitch,
+                                                          h->uz, h->uf, h->p.lmag);
+    CK(cudaGetLastError());
+    k_frad<<<1, 256, 0, h->st>>>(dout, h->m.dzzdz, h->m.rkapa, h->p.hz, h->p.repr, npz);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, sizeof(double) * MHD3D_NPROF * npz, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
 }  // namespace
 }  // namespace mhd3d
 
@@ -1027,6 +1142,12 @@ int mhd3d_fluxes(void* handle, double* fu, double* fv, double* fw, double* fr, d
     if (!handle) return MHD3D_ERR_ARG;
     double* o[8] = {fu, fv, fw, fr, ft, ww1, ww2, ww3};
     return fluxes(static_cast<Handle*>(handle), o);
+}
+
+int mhd3d_profiles(void* handle, double* out)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    return profiles(static_cast<Handle*>(handle), out);
 }
 
 int mhd3d_cfl(void* handle, double* dt, double* umach)

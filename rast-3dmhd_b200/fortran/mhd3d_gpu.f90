@@ -12,6 +12,8 @@ module mhd3d_gpu
        MHD3D_ERR_NONFINITE = 3, MHD3D_ERR_DT_SMALL = 4, MHD3D_ERR_NO_DEVICE = 5, &
        MHD3D_ERR_TIMEOUT = 6, MHD3D_ERR_NOMEM = 7
   integer(c_int), parameter :: MHD3D_MODE_EXACT = 0, MHD3D_MODE_FAST = 1, MHD3D_MODE_FP32 = 2
+  integer(c_int), parameter :: MHD3D_NPROF = 7, MHD3D_PROF_RHO = 0, MHD3D_PROF_T = 1, MHD3D_PROF_KE = 2, &
+       MHD3D_PROF_ENTH = 3, MHD3D_PROF_FCONV = 4, MHD3D_PROF_FRAD = 5, MHD3D_PROF_ME = 6
 
   type, bind(C) :: mhd3d_params
      integer(c_int32_t) :: npx, npy, npz
@@ -76,5 +78,12 @@ module mhd3d_gpu
        import :: c_int, c_ptr
        type(c_ptr), value :: handle
      end function mhd3d_bcon
+
+     ! PROF(NPZ, MHD3D_NPROF): column r+1 holds row MHD3D_PROF_* = r for K=2..NZ-1
+     integer(c_int) function mhd3d_profiles(handle, prof) bind(C, name="mhd3d_profiles")
+       import :: c_int, c_double, c_ptr
+       type(c_ptr), value :: handle
+       real(c_double), intent(out) :: prof(*)
+     end function mhd3d_profiles
   end interface
 end module mhd3d_gpu

@@ -23,6 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 FIELDS = ("ru", "rv", "rw", "tt", "ro", "bx", "by", "bz")
 FLUXES = ("fu", "fv", "fw", "fr", "ft", "ww1", "ww2", "ww3")
+# rows of mhd3d_profiles (MHD3D_PROF_*)
+PROFILES = ("rho", "t", "ke", "enth", "fconv", "frad", "me")
 
 MODE_EXACT = 0
 MODE_FAST = 1
@@ -103,6 +105,7 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_fluxes.argtypes = [vp] + [vp] * 8
     lib.mhd3d_cfl.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.mhd3d_bcon.argtypes = [vp]
+    lib.mhd3d_profiles.argtypes = [vp, vp]
     lib.mhd3d_version.restype = C.c_char_p
     lib.mhd3d_set_stream.argtypes = [vp, vp]
     lib.mhd3d_step_async.argtypes = [vp, C.c_int32]
@@ -279,6 +282,14 @@ class GpuSim:
         st = self.lib.mhd3d_fluxes(self.h, *[_ptr(out[f]) for f in FLUXES])
         if st:
             raise Mhd3dError(st, "mhd3d_fluxes")
+        return out
+
+    def profiles(self) -> np.ndarray:
+        """Horizontal-mean profiles (rows PROFILES) over the interior planes K=2..NZ-1."""
+        out = np.zeros((len(PROFILES), self.params.npz))
+        st = self.lib.mhd3d_profiles(self.h, out.ctypes.data_as(C.c_void_p))
+        if st:
+            raise Mhd3dError(st, "mhd3d_profiles")
         return out
 
     def cfl(self):

@@ -1,8 +1,8 @@
 """Generate the golden fixtures of the time step from the reference's own code.
 
 The reference has no tests or golden data.  These fixtures come from its
-STEP/FLUXES/BCON/COMMUNICATE source, translated mechanically to C and run
-with its own MPI decomposition (oracle/make_ref.py builds oracle/_ref/ref3dmhd
+STEP/FLUXES/BCON/COMMUNICATE/HORIZONTAL_MEAN source, translated mechanically
+to C and run with its own MPI decomposition (oracle/make_ref.py builds oracle/_ref/ref3dmhd
 from the reference checkout).  Each fixture holds the inputs (COMMON scalars,
 metric arrays, the state in Fortran layout) and the reference's outputs, so
 tests can pin the CPU oracle without the reference checkout.
@@ -90,6 +90,9 @@ def main():
             arrs["out_" + f] = res[f]
         for f in oracle_py.FLUXES[:nf]:
             arrs["flux_" + f] = flux[f]
+        # horizontal-mean profiles by the reference's HORIZONTAL_MEAN (one y rank:
+        # with more, the reference's own sum over y ranks rounds differently)
+        arrs["profiles"] = oracle_py.run_reference(p, setup.grid, state, 0, npey=1, npez=npez, mode=2)["profiles"]
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **arrs)
         print(path, os.path.getsize(path))

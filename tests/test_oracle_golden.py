@@ -50,3 +50,10 @@ def test_oracle_matches_reference_fluxes(path, mhd3d, oracle):
     sl = (slice(1, -1),) * 3
     for f in mhd3d.FLUXES[: len(fields)]:
         assert np.array_equal(fl[f][sl], z["flux_" + f][sl]), f
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(g)[:-4] for g in GOLDEN])
+def test_oracle_matches_reference_profiles(path, mhd3d, oracle):
+    z, p, grid, st_in, fields = _load(path, mhd3d)
+    o = oracle.Oracle(p, grid, st_in)
+    assert np.array_equal(o.profiles(), z["profiles"])
