@@ -248,6 +248,32 @@ int mhd3d_cfl_noalloc(const mhd3d_params* p,
                       double* out, void* stream);
 
 /* Version string of the library. */
+/*
+ * Batched ensemble (no counterpart in the reference): nmembers independent
+ * FP32 grids of any sizes (params[i].mode must be MHD3D_MODE_FP32; LMAG and
+ * LROT equal across members), stepped together.  Each RK3 stage of all
+ * members is one persistent launch over a work table (member, tile, z
+ * chunk), largest members first; a step is one CUDA graph.  grids holds
+ * 14*nmembers pointers, the mhd3d_create metric arrays of each member in
+ * turn.  Members keep their own DT, TIMT, NIT and stop status.
+ *
+ * mhd3d_ensemble_member returns member i's handle for mhd3d_upload,
+ * mhd3d_download, mhd3d_profiles and mhd3d_cfl; it stays owned by the
+ * ensemble (never pass it to mhd3d_destroy).  mhd3d_ensemble_step enqueues
+ * nsteps steps of every member without waiting; mhd3d_ensemble_sync waits
+ * and returns per-member DT, TIMT, NIT and status (arrays of nmembers; any
+ * may be NULL) and the first non-zero status.  mhd3d_ensemble_tune times
+ * `steps` steps for each z-chunk length in {4,6,8,12,16,24,32,48,64} and
+ * persistent CTAs per SM in {2,3,4} on the current state, restores the
+ * state, and keeps the fastest pair.
+ */
+int mhd3d_ensemble_create(int32_t nmembers, const mhd3d_params* params, const double* const* grids, void** ens);
+int mhd3d_ensemble_destroy(void* ens);
+int mhd3d_ensemble_member(void* ens, int32_t i, void** handle);
+int mhd3d_ensemble_step(void* ens, int32_t nsteps);
+int mhd3d_ensemble_sync(void* ens, double* dt, double* timt, int32_t* nit, int32_t* status);
+int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_per_sm, double* ms_per_step);
+
 const char* mhd3d_version(void);
 
 #ifdef __cplusplus

@@ -293,8 +293,8 @@ __global__ void k_reset(Control* ctl, Accum* acc, int clear_stop, unsigned long 
 // End of a step (advance=1: NIT, TIMC, TIMT of STEP 3dmhdsub.f:1171-1173 and
 // the driver's DT check 3dmhd.f:924) and DT/UMACH of the next step from the
 // CFL accumulators (DT=SF*MIN(...), 3dmhdsub.f:866-873; UMACH=SQRT(...), 761).
-__global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance,
-                           unsigned long long w4key)
+__device__ void finalize_one(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance,
+                             unsigned long long w4key)
 {
     if (advance) {
         if (ctl->stop) return;
@@ -323,6 +323,26 @@ __global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, in
     acc->wmin[3] = w4key;
     acc->umax = 0ull;
     acc->bad = 0u;
+}
+
+__global__ void k_finalize(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance,
+                           unsigned long long w4key)
+{
+    finalize_one(ctl, acc, sf, dtmin, lmag, advance, w4key);
+}
+
+// end of a step of every member of an ensemble (one thread per member)
+struct FinArgs {
+    Control* ctl;
+    Accum* acc;
+    double sf, dtmin;
+    unsigned long long w4key;
+    int lmag, pad;
+};
+__global__ void k_finalize_multi(const FinArgs* __restrict__ f, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) finalize_one(f[i].ctl, f[i].acc, f[i].sf, f[i].dtmin, f[i].lmag, 1, f[i].w4key);
 }
 
 unsigned grid_for(size_t n)
@@ -1031,6 +1051,308 @@ int profiles(Handle* h, double* out)
     return MHD3D_OK;
 }
 
+// ---- batched ensemble of FP32 grids ---------------------------------------
+// Members are ordinary FP32 handles on one stream.  Each RK3 stage of every
+// member runs in ONE persistent launch (f32::launch_stage_multi) over a work
+// table (member, tile, z chunk), largest members first; k_finalize_multi
+// ends the step of all members; one step is one CUDA graph (two graphs,
+// for the two ping-pong parities of a step).  The member arguments live in
+// device tables that each call refreshes, so the graphs never need
+// re-capturing while the decomposition is unchanged.
+struct Ensemble {
+    std::vector<Handle*> mem;
+    cudaStream_t st = nullptr;
+    int dev = -1, lmag = 0, lrot = 0, sms = 148;
+    int ctas_per_sm = 4;                    // persistent CTAs per SM
+    StageArgs32* dargs[2] = {nullptr, nullptr};
+    int* dorder = nullptr;                  // members by decreasing work
+    int* dbase = nullptr;                   // first item of each member in that order (+ total)
+    unsigned* dcount = nullptr;             // work counters of the three stages
+    FinArgs* dfin = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<int> order;
+    int nitems = 0;
+};
+
+int ens_destroy(Ensemble* e)
+{
+    if (!e) return MHD3D_OK;
+    if (e->dev >= 0) cudaSetDevice(e->dev);
+    for (int q = 0; q < 2; ++q) {
+        if (e->graph[q]) cudaGraphExecDestroy(e->graph[q]);
+        cudaFree(e->dargs[q]);
+    }
+    cudaFree(e->dorder);
+    cudaFree(e->dbase);
+    cudaFree(e->dcount);
+    cudaFree(e->dfin);
+    for (Handle* h : e->mem) destroy(h);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
+    return MHD3D_OK;
+}
+
+// work table: member order (largest first) and item prefix sums
+int ens_layout(Ensemble* e)
+{
+    const int n = (int)e->mem.size();
+    std::vector<long> items(n);
+    for (int i = 0; i < n; ++i) {
+        Handle* h = e->mem[i];
+        items[i] = (long)h->ntx * ((h->p.npy + TY32 - 1) / TY32) * h->nchunks;
+    }
+    e->order.resize(n);
+    for (int i = 0; i < n; ++i) e->order[i] = i;
+    std::stable_sort(e->order.begin(), e->order.end(), [&](int a, int b) { return items[a] > items[b]; });
+    std::vector<int> base(n + 1, 0);
+    for (int i = 0; i < n; ++i) base[i + 1] = base[i] + (int)items[e->order[i]];
+    e->nitems = base[n];
+    CK(cudaMemcpyAsync(e->dorder, e->order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(e->dbase, base.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    for (int q = 0; q < 2; ++q)
+        if (e->graph[q]) {
+            cudaGraphExecDestroy(e->graph[q]);
+            e->graph[q] = nullptr;
+        }
+    return MHD3D_OK;
+}
+
+int ens_create(int n, const mhd3d_params* ps, const double* const* grids, Ensemble** out)
+{
+    if (n < 1 || !ps || !grids) return MHD3D_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (ps[i].mode != MHD3D_MODE_FP32 || ps[i].lmag != ps[0].lmag || ps[i].lrot != ps[0].lrot)
+            return MHD3D_ERR_ARG;
+    Ensemble* e = new (std::nothrow) Ensemble();
+    if (!e) return MHD3D_ERR_NOMEM;
+    *out = e;
+    CK(cudaGetDevice(&e->dev));
+    CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+    cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->dev);
+    e->lmag = ps[0].lmag;
+    e->lrot = ps[0].lrot;
+    e->mem.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        void* hv = nullptr;
+        int st = create(&ps[i], grids + 14 * (size_t)i, &hv);
+        e->mem[i] = static_cast<Handle*>(hv);
+        if (st) return st;
+        e->mem[i]->st = e->st;   // every member works on the ensemble's stream
+    }
+    for (int q = 0; q < 2; ++q) CK(cudaMalloc(&e->dargs[q], sizeof(StageArgs32) * n));
+    CK(cudaMalloc(&e->dorder, sizeof(int) * n));
+    CK(cudaMalloc(&e->dbase, sizeof(int) * (n + 1)));
+    CK(cudaMalloc(&e->dcount, sizeof(unsigned) * 4));
+    CK(cudaMalloc(&e->dfin, sizeof(FinArgs) * n));
+    std::vector<FinArgs> fin(n);
+    for (int i = 0; i < n; ++i) {
+        Handle* h = e->mem[i];
+        fin[i] = FinArgs{h->ctl, h->acc, h->s.sf, h->s.dtmin, h->w4key, h->p.lmag, 0};
+    }
+    CK(cudaMemcpy(e->dfin, fin.data(), sizeof(FinArgs) * n, cudaMemcpyHostToDevice));
+    for (int stg = 1; stg <= 3; ++stg)   // kernel attributes are set outside any graph capture
+        CK(f32::launch_stage_multi(stg, e->lmag, e->lrot, nullptr, nullptr, nullptr, 0, nullptr, 0, e->st));
+    return ens_layout(e);
+}
+
+// set every member's z chunk length (<= 0: the single-grid default) and re-lay the work table
+int ens_set_zlen(Ensemble* e, int zlen)
+{
+    for (Handle* h : e->mem) {
+        const int npz = h->p.npz;
+        int nch;
+        if (zlen > 0) nch = std::max(1, npz / std::max(zlen, 3));
+        else nch = std::max(1, (npz + MHD3D_ZCHUNK - 1) / MHD3D_ZCHUNK);
+        while (nch > 1 && npz / nch < 3) --nch;
+        h->nchunks = nch;
+        h->zlen = npz / nch;
+    }
+    return ens_layout(e);
+}
+
+int ens_capture(Ensemble* e, int q)
+{
+    // a step whose stage 1 reads table q: stages use tables q, q^1, q
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    const int nb = std::max(1, std::min(e->nitems, e->sms * e->ctas_per_sm));
+    const int n = (int)e->mem.size();
+    cudaError_t err = cudaMemsetAsync(e->dcount, 0, sizeof(unsigned) * 4, e->st);
+    for (int stg = 1; stg <= 3 && err == cudaSuccess; ++stg)
+        err = f32::launch_stage_multi(stg, e->lmag, e->lrot, e->dargs[(stg == 2) ? (q ^ 1) : q], e->dorder,
+                                      e->dbase, n, e->dcount + (stg - 1), nb, e->st);
+    if (err == cudaSuccess) {
+        k_finalize_multi<<<(n + 127) / 128, 128, 0, e->st>>>(e->dfin, n);
+        err = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamEndCapture(e->st, &g);
+    if (err != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        CK(err != cudaSuccess ? err : e2);
+    }
+    err = cudaGraphInstantiate(&e->graph[q], g, 0);
+    cudaGraphDestroy(g);
+    CK(err);
+    return MHD3D_OK;
+}
+
+int ens_step(Ensemble* e, int nsteps)
+{
+    CK(cudaSetDevice(e->dev));
+    if (nsteps < 0) return MHD3D_ERR_ARG;
+    const int n = (int)e->mem.size();
+    std::vector<StageArgs32> tab[2];
+    tab[0].resize(n);
+    tab[1].resize(n);
+    std::vector<int> cur0(n);
+    for (int i = 0; i < n; ++i) {
+        Handle* h = e->mem[i];
+        if (!h->dt_valid) {
+            int st = initial_dt(h);
+            if (st) return st;
+        } else if (h->pending == 0) {
+            k_reset<<<1, 1, 0, h->st>>>(h->ctl, h->acc, 1, h->w4key);
+            CK(cudaGetLastError());
+        }
+        const int cur = h->cur_base ^ (h->pending & 1);
+        cur0[i] = cur;
+        for (int p = 0; p < 2; ++p) {
+            StageArgs32 a = make_args32(h);
+            const int in = cur ^ p;
+            a.map_u = h->map_u[in];
+            a.u_in = reinterpret_cast<const float*>(h->ubuf[in]);
+            a.u_out = reinterpret_cast<float*>(h->ubuf[in ^ 1]);
+            tab[p][i] = a;
+        }
+    }
+    for (int p = 0; p < 2; ++p)
+        CK(cudaMemcpyAsync(e->dargs[p], tab[p].data(), sizeof(StageArgs32) * n, cudaMemcpyHostToDevice, e->st));
+    for (int q = 0; q < 2; ++q)
+        if (!e->graph[q]) {
+            int st = ens_capture(e, q);
+            if (st) return st;
+        }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(e->graph[s & 1], e->st));
+    for (int i = 0; i < n; ++i) {
+        Handle* h = e->mem[i];
+        h->pending += nsteps;
+        h->cur = cur0[i] ^ (nsteps & 1);
+    }
+    return MHD3D_OK;
+}
+
+int ens_sync(Ensemble* e, double* dt, double* timt, int32_t* nit, int32_t* status)
+{
+    CK(cudaSetDevice(e->dev));
+    int worst = MHD3D_OK;
+    for (size_t i = 0; i < e->mem.size(); ++i) {
+        double d = 0, tc = 0, tt = 0, um = 0;
+        int32_t ni = 0;
+        const int st = sync(e->mem[i], &d, &tc, &tt, &um, &ni);
+        if (dt) dt[i] = d;
+        if (timt) timt[i] = tt;
+        if (nit) nit[i] = ni;
+        if (status) status[i] = st;
+        if (st == MHD3D_ERR_CUDA) return st;
+        if (st && !worst) worst = st;
+    }
+    return worst;
+}
+
+// Autotuner: time a few steps for each (z chunk length, persistent CTAs per
+// SM) pair on the live state, keep the fastest, and put the state back.
+int ens_tune(Ensemble* e, int steps, int32_t* zlen_out, int32_t* ctas_out, double* ms_out)
+{
+    CK(cudaSetDevice(e->dev));
+    if (int st = ens_sync(e, nullptr, nullptr, nullptr, nullptr)) {
+        if (st == MHD3D_ERR_CUDA) return st;
+    }
+    const int n = (int)e->mem.size();
+    int maxnpz = 0;
+    for (Handle* h : e->mem) maxnpz = std::max(maxnpz, h->p.npz);
+    // snapshot: both U buffers, Control, Accum of every member
+    std::vector<void*> snap(n, nullptr);
+    std::vector<size_t> ubytes(n);
+    for (int i = 0; i < n; ++i) {
+        Handle* h = e->mem[i];
+        ubytes[i] = (h->f32 ? sizeof(float) : sizeof(double)) * h->nf * h->uf;
+        CK(cudaMalloc(&snap[i], 2 * ubytes[i] + sizeof(Control) + sizeof(Accum)));
+        char* b = static_cast<char*>(snap[i]);
+        CK(cudaMemcpyAsync(b, h->ubuf[0], ubytes[i], cudaMemcpyDeviceToDevice, e->st));
+        CK(cudaMemcpyAsync(b + ubytes[i], h->ubuf[1], ubytes[i], cudaMemcpyDeviceToDevice, e->st));
+        CK(cudaMemcpyAsync(b + 2 * ubytes[i], h->ctl, sizeof(Control), cudaMemcpyDeviceToDevice, e->st));
+        CK(cudaMemcpyAsync(b + 2 * ubytes[i] + sizeof(Control), h->acc, sizeof(Accum), cudaMemcpyDeviceToDevice,
+                           e->st));
+    }
+    std::vector<int> saved_cur(n), saved_base(n), saved_nit(n), saved_valid(n);
+    for (int i = 0; i < n; ++i) {
+        saved_cur[i] = e->mem[i]->cur;
+        saved_base[i] = e->mem[i]->cur_base;
+        saved_nit[i] = e->mem[i]->nit_base;
+        saved_valid[i] = e->mem[i]->dt_valid;
+    }
+    auto restore = [&]() -> int {
+        for (int i = 0; i < n; ++i) {
+            Handle* h = e->mem[i];
+            char* b = static_cast<char*>(snap[i]);
+            CK(cudaMemcpyAsync(h->ubuf[0], b, ubytes[i], cudaMemcpyDeviceToDevice, e->st));
+            CK(cudaMemcpyAsync(h->ubuf[1], b + ubytes[i], ubytes[i], cudaMemcpyDeviceToDevice, e->st));
+            CK(cudaMemcpyAsync(h->ctl, b + 2 * ubytes[i], sizeof(Control), cudaMemcpyDeviceToDevice, e->st));
+            CK(cudaMemcpyAsync(h->acc, b + 2 * ubytes[i] + sizeof(Control), sizeof(Accum), cudaMemcpyDeviceToDevice,
+                               e->st));
+            h->cur = saved_cur[i];
+            h->cur_base = saved_base[i];
+            h->nit_base = saved_nit[i];
+            h->pending = 0;
+            h->dt_valid = saved_valid[i];
+        }
+        CK(cudaStreamSynchronize(e->st));
+        return MHD3D_OK;
+    };
+    const int zc[] = {4, 6, 8, 12, 16, 24, 32, 48, 64};
+    const int cc[] = {2, 3, 4};
+    int best_z = 0, best_c = e->ctas_per_sm;
+    double best = 1e300;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    int st = MHD3D_OK;
+    for (int zi = 0; zi < (int)(sizeof(zc) / sizeof(zc[0])) && !st; ++zi) {
+        if (zc[zi] > maxnpz) break;
+        for (int ci = 0; ci < 3 && !st; ++ci) {
+            e->ctas_per_sm = cc[ci];
+            if ((st = ens_set_zlen(e, zc[zi]))) break;
+            if ((st = ens_step(e, 1))) break;   // warm-up, builds the graphs
+            cudaEventRecord(t0, e->st);
+            if ((st = ens_step(e, steps))) break;
+            cudaEventRecord(t1, e->st);
+            if (cudaEventSynchronize(t1) != cudaSuccess) { st = MHD3D_ERR_CUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            if ((st = restore())) break;
+            const double per = ms / std::max(steps, 1);
+            if (per < best) {
+                best = per;
+                best_z = zc[zi];
+                best_c = cc[ci];
+            }
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    int st2 = restore();
+    for (void* p : snap) cudaFree(p);
+    if (st) return st;
+    if (st2) return st2;
+    e->ctas_per_sm = best_c;
+    if (int s3 = ens_set_zlen(e, best_z)) return s3;
+    if (zlen_out) *zlen_out = best_z;
+    if (ctas_out) *ctas_out = best_c;
+    if (ms_out) *ms_out = best;
+    return MHD3D_OK;
+}
+
 }  // namespace
 }  // namespace mhd3d
 
@@ -1178,6 +1500,48 @@ int mhd3d_bcon(void* handle)
     CK(cudaStreamSynchronize(h->st));
     h->dt_valid = false;
     return MHD3D_OK;
+}
+
+int mhd3d_ensemble_create(int32_t nmembers, const mhd3d_params* params, const double* const* grids, void** ens)
+{
+    if (!ens) return MHD3D_ERR_ARG;
+    *ens = nullptr;
+    Ensemble* e = nullptr;
+    int st = ens_create(nmembers, params, grids, &e);
+    if (st) {
+        ens_destroy(e);
+        return st;
+    }
+    *ens = e;
+    return MHD3D_OK;
+}
+
+int mhd3d_ensemble_destroy(void* ens) { return ens_destroy(static_cast<Ensemble*>(ens)); }
+
+int mhd3d_ensemble_member(void* ens, int32_t i, void** handle)
+{
+    Ensemble* e = static_cast<Ensemble*>(ens);
+    if (!e || !handle || i < 0 || i >= (int)e->mem.size()) return MHD3D_ERR_ARG;
+    *handle = e->mem[i];
+    return MHD3D_OK;
+}
+
+int mhd3d_ensemble_step(void* ens, int32_t nsteps)
+{
+    if (!ens) return MHD3D_ERR_ARG;
+    return ens_step(static_cast<Ensemble*>(ens), nsteps);
+}
+
+int mhd3d_ensemble_sync(void* ens, double* dt, double* timt, int32_t* nit, int32_t* status)
+{
+    if (!ens) return MHD3D_ERR_ARG;
+    return ens_sync(static_cast<Ensemble*>(ens), dt, timt, nit, status);
+}
+
+int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_per_sm, double* ms_per_step)
+{
+    if (!ens || steps < 1) return MHD3D_ERR_ARG;
+    return ens_tune(static_cast<Ensemble*>(ens), steps, zlen, ctas_per_sm, ms_per_step);
 }
 
 const char* mhd3d_version(void) { return "mhd3d-b200 0.2 (sm_100a, FP64 exact/FMA, FP32 perturbation form)"; }

@@ -216,6 +216,10 @@ namespace f32 {
 size_t stage_smem_bytes(int lmag);
 cudaError_t launch_stage(int stage, const StageArgs32& a, cudaStream_t st);
 cudaError_t launch_cfl(const StageArgs32& a, cudaStream_t st);
+// persistent multi-grid form (ensembles): args, order, item_base in device memory;
+// nblocks == 0 only prepares the kernel attributes (before a graph capture)
+cudaError_t launch_stage_multi(int stage, int lmag, int lrot, const StageArgs32* args, const int* order,
+                               const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st);
 }
 
 }  // namespace mhd3d

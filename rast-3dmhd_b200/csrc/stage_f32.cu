@@ -144,13 +144,16 @@ __device__ __forceinline__ void cfl32_commit(Accum* acc, unsigned long long* red
 #define MHD3D_MINB32 5   // 5 x 128 threads x 96 registers, 5 x 34 KB shared
 #endif
 
+// One work item: the z chunk `chunk` of tile `tile` of the grid described by
+// `a`, on the CTA's shared memory `sb` (128-byte aligned).  On return every
+// TMA copy the item issued has landed and its mbarriers are invalidated, so
+// a persistent CTA can take the next item.
 template <bool MAG, bool ROT, int STAGE>
-__global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_constant__ StageArgs32 a)
+__device__ __forceinline__ void stage32_item(const StageArgs32& a, const int tile, const int chunk,
+                                             unsigned char* const sb)
 {
     using L = Lay32<MAG>;
     constexpr int NF = L::NF;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     float* const sraw = reinterpret_cast<float*>(sb);
     float* const sri = reinterpret_cast<float*>(sb + L::RI_OFF_B);
     float* const sz = reinterpret_cast<float*>(sb + L::Z_OFF_B);
@@ -159,16 +162,12 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
     int* const sflag = reinterpret_cast<int*>(sb + L::FLAG_OFF_B);
 
     const Control* ctl = a.ctl;
-    if (STAGE != 0 && ctl->stop) return;
-
     const Scalars& s = a.s;
     const Metrics& m = a.m;
     const int npx = s.npx, npy = s.npy, npz = s.npz;
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    const int tile = blockIdx.x;
     const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY32;
-    const int chunk = blockIdx.y;
     const int k0 = chunk * a.zlen;
     const int k1 = (chunk == a.nchunks - 1) ? npz : k0 + a.zlen;
     const int gi = x0 + tx, gj = y0 + ty;
@@ -194,10 +193,14 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
     const size_t zcol = (size_t)gj * a.zpitch + gi;
     const HaloCols hc = halo_cols(npx, npy, a.upitch, gi, gj);
 
+    // the stop flag is read once, by one thread, so the CTA takes one path
     if (tid == 0) {
-        for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
-        *sflag = 0;
-        fence_mbar_init();
+        const bool stopped = STAGE != 0 && ctl->stop;
+        *sflag = stopped ? -1 : 0;
+        if (!stopped) {
+            for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
+            fence_mbar_init();
+        }
     }
     if (STAGE == 3 && (tid & 31) == 0) {
         unsigned long long* r = red + (tid >> 5) * 3;
@@ -206,6 +209,7 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
         r[2] = 0ull;
     }
     __syncthreads();
+    if (*sflag < 0) return;
 
     int hi_issued = k0 - 2;
     auto issue_plane = [&](int kp) {
@@ -575,9 +579,58 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
             atomicExch(&a.ctl->status, MHD3D_ERR_TIMEOUT);
             atomicExch(&a.ctl->stop, 1);
         }
-        return;
+    } else if (STAGE == 3) {
+        cfl32_commit(a.acc, red, cfa);
     }
-    if (STAGE == 3) cfl32_commit(a.acc, red, cfa);
+    __syncthreads();
+    if (tid == 0)
+        for (int i = 0; i < NRAW + 1; ++i) mbar_inval(&bars[i]);
+}
+
+template <bool MAG, bool ROT, int STAGE>
+__global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_constant__ StageArgs32 a)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    stage32_item<MAG, ROT, STAGE>(a, blockIdx.x, blockIdx.y, sb);
+}
+
+// Persistent form for an ensemble of grids: one launch per RK3 stage for all
+// members.  Work items (member, tile, z chunk) are numbered member by member
+// in `order` (largest members first); item_base[i] is the first item of the
+// i-th member in that order.  CTAs take items from a global counter until
+// none is left, so members of uneven size share the SMs.
+#ifndef MHD3D_MINB32M
+#define MHD3D_MINB32M 4   // the persistent form carries its loop state as well: 128 registers, no spills
+#endif
+template <bool MAG, bool ROT, int STAGE>
+__global__ void __launch_bounds__(NT32, MHD3D_MINB32M) k_stage32_multi(const StageArgs32* __restrict__ args,
+                                                                      const int* __restrict__ order,
+                                                                      const int* __restrict__ item_base, int nmem,
+                                                                      unsigned* counter)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    __shared__ int s_item;
+    const int nitems = item_base[nmem];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= nitems) break;
+        int lo = 0, hi = nmem - 1;   // last i with item_base[i] <= it
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (item_base[mid] <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        const StageArgs32& a = args[order[lo]];
+        const int ntiles = a.ntx * ((a.s.npy + TY32 - 1) / TY32);
+        const int local = it - item_base[lo];
+        stage32_item<MAG, ROT, STAGE>(a, local % ntiles, local / ntiles, sb);
+        __syncthreads();
+    }
 }
 
 // CFL reduction over the current FP32 state, formed in FP64 (first step,
@@ -669,6 +722,43 @@ cudaError_t launch_stage(int stage, const StageArgs32& a, cudaStream_t st)
 }
 
 size_t stage_smem_bytes(int lmag) { return lmag ? Lay32<true>::BYTES : Lay32<false>::BYTES; }
+
+template <bool MAG, bool ROT>
+static cudaError_t launch_multi_t(int stage, const StageArgs32* args, const int* order, const int* item_base,
+                                  int nmem, unsigned* counter, int nblocks, cudaStream_t st)
+{
+    const size_t smem = Lay32<MAG>::BYTES;
+    switch (stage) {
+#define L_(S)                                                                                              \
+    case S: {                                                                                              \
+        static bool attr_set = false;                                                                      \
+        if (!attr_set) {                                                                                   \
+            cudaError_t e = cudaFuncSetAttribute(k_stage32_multi<MAG, ROT, S>,                             \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+            if (e != cudaSuccess) return e;                                                                \
+            attr_set = true;                                                                               \
+        }                                                                                                  \
+        if (nblocks > 0)                                                                                   \
+            k_stage32_multi<MAG, ROT, S><<<nblocks, NT32, smem, st>>>(args, order, item_base, nmem, counter); \
+        break;                                                                                             \
+    }
+        L_(1) L_(2) L_(3)
+#undef L_
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage_multi(int stage, int lmag, int lrot, const StageArgs32* args, const int* order,
+                               const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st)
+{
+    if (lmag)
+        return lrot ? launch_multi_t<true, true>(stage, args, order, item_base, nmem, counter, nblocks, st)
+                    : launch_multi_t<true, false>(stage, args, order, item_base, nmem, counter, nblocks, st);
+    return lrot ? launch_multi_t<false, true>(stage, args, order, item_base, nmem, counter, nblocks, st)
+                : launch_multi_t<false, false>(stage, args, order, item_base, nmem, counter, nblocks, st);
+}
 
 cudaError_t launch_cfl(const StageArgs32& a, cudaStream_t st)
 {

@@ -155,7 +155,6 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     int* const sflag = reinterpret_cast<int*>(sbase + L::FLAG_OFF);
 
     const Control* ctl = a.ctl;
-    if (STAGE != 0 && ctl->stop) return;
 
     const Scalars& s = a.s;
     const Metrics& m = a.m;
@@ -194,10 +193,14 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     const size_t zcol = (size_t)gj * a.zpitch + gi;
     const HaloCols hc = halo_cols(npx, npy, a.upitch, gi, gj);
 
+    // the stop flag is read once, by one thread, so the CTA takes one path
     if (tid == 0) {
-        for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
-        *sflag = 0;
-        fence_mbar_init();
+        const bool stopped = STAGE != 0 && ctl->stop;
+        *sflag = stopped ? -1 : 0;
+        if (!stopped) {
+            for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
+            fence_mbar_init();
+        }
     }
     if (STAGE == 3 && (tid & 31) == 0) {
         unsigned long long* r = red + (tid >> 5) * 3;
@@ -206,6 +209,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         r[2] = 0ull;
     }
     __syncthreads();
+    if (*sflag < 0) return;
 
     // plane kp (-1 .. npz) lives in raw slot (kp+1)&3 and 1/RO slot (kp+1)%3;
     // it is the ((kp-(k0-1))>>2)-th fill of its slot

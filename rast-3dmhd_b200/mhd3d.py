@@ -106,6 +106,13 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_cfl.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.mhd3d_bcon.argtypes = [vp]
     lib.mhd3d_profiles.argtypes = [vp, vp]
+    lib.mhd3d_ensemble_create.argtypes = [C.c_int32, C.POINTER(Params), C.POINTER(vp), C.POINTER(vp)]
+    lib.mhd3d_ensemble_destroy.argtypes = [vp]
+    lib.mhd3d_ensemble_member.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+    lib.mhd3d_ensemble_step.argtypes = [vp, C.c_int32]
+    lib.mhd3d_ensemble_sync.argtypes = [vp, vp, vp, vp, vp]
+    lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_double)]
     lib.mhd3d_version.restype = C.c_char_p
     lib.mhd3d_set_stream.argtypes = [vp, vp]
     lib.mhd3d_step_async.argtypes = [vp, C.c_int32]
@@ -195,22 +202,26 @@ def wrap_periodic(a: np.ndarray) -> np.ndarray:
 class GpuSim:
     """A handle of the GPU time-step library (one per simulation)."""
 
-    def __init__(self, setup: Setup, mode: int | None = None):
+    def __init__(self, setup: Setup, mode: int | None = None, _handle: C.c_void_p | None = None):
         self.lib = gpu_lib()
         self.setup = setup
         p = Params.from_buffer_copy(setup.params)
         if mode is not None:
             p.mode = mode
         self.params = p
+        self.owned = _handle is None
+        if _handle is not None:   # a member of an Ensemble, owned by it
+            self.h = _handle
+            return
         self.h = C.c_void_p()
         st = self.lib.mhd3d_create(C.byref(p), *setup.grid_args(), C.byref(self.h))
         if st:
             raise Mhd3dError(st, "mhd3d_create")
 
     def close(self):
-        if self.h:
+        if self.h and self.owned:
             self.lib.mhd3d_destroy(self.h)
-            self.h = C.c_void_p()
+        self.h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -303,3 +314,71 @@ class GpuSim:
         st = self.lib.mhd3d_bcon(self.h)
         if st:
             raise Mhd3dError(st, "mhd3d_bcon")
+
+
+class Ensemble:
+    """A batched ensemble of FP32 grids (mhd3d_ensemble_*): one persistent
+    launch per RK3 stage for all members, one CUDA graph per step."""
+
+    def __init__(self, setups: list):
+        self.lib = gpu_lib()
+        n = len(setups)
+        self.setups = setups
+        ps = (Params * n)()
+        for i, su in enumerate(setups):
+            ps[i] = Params.from_buffer_copy(su.params)
+            ps[i].mode = MODE_FP32
+        grids = (C.c_void_p * (14 * n))()
+        for i, su in enumerate(setups):
+            for j, a in enumerate(su.grid_args()):
+                grids[14 * i + j] = a.value if isinstance(a, C.c_void_p) else a
+        self.h = C.c_void_p()
+        st = self.lib.mhd3d_ensemble_create(n, ps, grids, C.byref(self.h))
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_create")
+        self.members = []
+        for i, su in enumerate(setups):
+            mh = C.c_void_p()
+            st = self.lib.mhd3d_ensemble_member(self.h, i, C.byref(mh))
+            if st:
+                raise Mhd3dError(st, "mhd3d_ensemble_member")
+            self.members.append(GpuSim(su, mode=MODE_FP32, _handle=mh))
+
+    def close(self):
+        if self.h:
+            for m in self.members:
+                m.h = C.c_void_p()
+            self.lib.mhd3d_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step_async(self, n: int = 1):
+        st = self.lib.mhd3d_ensemble_step(self.h, n)
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_step")
+
+    def sync(self) -> dict:
+        n = len(self.members)
+        dt, timt = np.zeros(n), np.zeros(n)
+        nit, status = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        st = self.lib.mhd3d_ensemble_sync(self.h, dt.ctypes.data_as(C.c_void_p), timt.ctypes.data_as(C.c_void_p),
+                                          nit.ctypes.data_as(C.c_void_p), status.ctypes.data_as(C.c_void_p))
+        if st == 2:
+            raise Mhd3dError(st, "mhd3d_ensemble_sync")
+        return {"status": status, "dt": dt, "timt": timt, "nit": nit, "first_status": st}
+
+    def step(self, n: int = 1) -> dict:
+        self.step_async(n)
+        return self.sync()
+
+    def tune(self, steps: int = 3) -> dict:
+        z, c, ms = C.c_int32(), C.c_int32(), C.c_double()
+        st = self.lib.mhd3d_ensemble_tune(self.h, steps, C.byref(z), C.byref(c), C.byref(ms))
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_tune")
+        return {"zlen": z.value, "ctas_per_sm": c.value, "ms_per_step": ms.value}
