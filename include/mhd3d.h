@@ -273,6 +273,8 @@ int mhd3d_ensemble_member(void* ens, int32_t i, void** handle);
 int mhd3d_ensemble_step(void* ens, int32_t nsteps);
 int mhd3d_ensemble_sync(void* ens, double* dt, double* timt, int32_t* nit, int32_t* status);
 int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_per_sm, double* ms_per_step);
+/* enqueue the ensemble's work on a caller's cudaStream_t (NULL: its own) */
+int mhd3d_ensemble_set_stream(void* ens, void* stream);
 
 const char* mhd3d_version(void);
 

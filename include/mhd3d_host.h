@@ -93,6 +93,38 @@ int mhd3d_host_static(const mhd3d_run_config* c, const double* zee,
 /* RAN2 (3dmhdsub.f:3377-3410): one deviate; state is idum, iy, ir[97]. */
 double mhd3d_host_ran2(int32_t* idum, int32_t* iy, int32_t* ir);
 
+/*
+ * The reference driver's dump and restart files (3dmhd.f:284-363 restart,
+ * 505-524 and 912-1009 dumps), for hosts that are not the Fortran program.
+ *
+ * mhd3d_host_par1: the 96-value PAR1 record: IPAR(1:32) as reals (ipar15 =
+ * NCASE, NCASEP, NTOTAL, NSTEP0, NSTART; the rest from the config, NPE,
+ * NPEY and NIT) and PAR(1:64) from the config, with PAR1(63)=DT and
+ * PAR1(64), PAR1(65) as the driver sets them (TIMT, 0 at the last step,
+ * else TIMI, TIMC).
+ *
+ * mhd3d_host_write_dump: dump number ndump (0-based, the driver's NDUMP0)
+ * of a single-domain run: FOUT.dat0.0000 records nf*ndump+1.. (interior of
+ * each field, REAL*8, direct access without record markers), FOUT.par
+ * record ndump+1 (PAR1), and the dump's seven 80-character records of
+ * FOUT.lis.  Fields are Fortran (NPX+2, NPY+2, NPZ+2) arrays.
+ *
+ * mhd3d_host_read_dump: restart from dump nstart (the driver's NSTART,
+ * 1-based) written by a run with npey x npez ranks (FINP.dat0.NNNN per
+ * rank): checks the sizes against FINP.par as the driver does, returns the
+ * PAR1 record (TIMI = PAR1(64)+PAR1(65)) and the global fields with the
+ * periodic halos filled; z ghost planes take the wall planes' values.
+ */
+void mhd3d_host_par1(const mhd3d_run_config* c, const int32_t ipar15[5], int32_t npe, int32_t npey, int32_t nit,
+                     double dt, double par64, double par65, double par1[96]);
+int mhd3d_host_write_dump(const char* fout, int32_t ndump, const double par1[96], int32_t npx, int32_t npy,
+                          int32_t npz, int32_t lmag, const double* ru, const double* rv, const double* rw,
+                          const double* tt, const double* ro, const double* bx, const double* by, const double* bz,
+                          double timt, double timc, double umach, double dt);
+int mhd3d_host_read_dump(const char* finp, int32_t nstart, int32_t npey, int32_t npez, int32_t lmag, int32_t npx,
+                         int32_t npy, int32_t npz, double par1[96], double* ru, double* rv, double* rw, double* tt,
+                         double* ro, double* bx, double* by, double* bz);
+
 #ifdef __cplusplus
 }
 #endif

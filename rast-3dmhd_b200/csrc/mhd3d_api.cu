@@ -1070,6 +1070,7 @@ struct Ensemble {
     unsigned* dcount = nullptr;             // work counters of the three stages
     FinArgs* dfin = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaStream_t own_st = nullptr;          // the ensemble's own stream while a caller's is in use
     std::vector<int> order;
     int nitems = 0;
 };
@@ -1087,7 +1088,8 @@ int ens_destroy(Ensemble* e)
     cudaFree(e->dcount);
     cudaFree(e->dfin);
     for (Handle* h : e->mem) destroy(h);
-    if (e->st) cudaStreamDestroy(e->st);
+    if (e->own_st) cudaStreamDestroy(e->own_st);
+    else if (e->st) cudaStreamDestroy(e->st);
     delete e;
     return MHD3D_OK;
 }
@@ -1536,6 +1538,18 @@ int mhd3d_ensemble_sync(void* ens, double* dt, double* timt, int32_t* nit, int32
 {
     if (!ens) return MHD3D_ERR_ARG;
     return ens_sync(static_cast<Ensemble*>(ens), dt, timt, nit, status);
+}
+
+int mhd3d_ensemble_set_stream(void* ens, void* stream)
+{
+    Ensemble* e = static_cast<Ensemble*>(ens);
+    if (!e) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(e->dev));
+    CK(cudaStreamSynchronize(e->st));
+    if (!e->own_st) e->own_st = e->st;
+    e->st = stream ? static_cast<cudaStream_t>(stream) : e->own_st;
+    for (Handle* h : e->mem) h->st = e->st;
+    return MHD3D_OK;
 }
 
 int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_per_sm, double* ms_per_step)

@@ -90,6 +90,13 @@ def host_lib() -> C.CDLL:
     lib.mhd3d_host_default_config.argtypes = [C.POINTER(RunConfig), C.c_int32, C.c_int32, C.c_int32]
     lib.mhd3d_host_ran2.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.mhd3d_host_ran2.restype = C.c_double
+    vp = C.c_void_p
+    lib.mhd3d_host_par1.argtypes = [C.POINTER(RunConfig), vp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                    C.c_double, C.c_double, vp]
+    lib.mhd3d_host_write_dump.argtypes = [C.c_char_p, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + \
+        [vp] * 8 + [C.c_double] * 4
+    lib.mhd3d_host_read_dump.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                         C.c_int32, C.c_int32, vp] + [vp] * 8
     return lib
 
 
@@ -111,6 +118,7 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_ensemble_member.argtypes = [vp, C.c_int32, C.POINTER(vp)]
     lib.mhd3d_ensemble_step.argtypes = [vp, C.c_int32]
     lib.mhd3d_ensemble_sync.argtypes = [vp, vp, vp, vp, vp]
+    lib.mhd3d_ensemble_set_stream.argtypes = [vp, vp]
     lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_double)]
     lib.mhd3d_version.restype = C.c_char_p
@@ -376,9 +384,49 @@ class Ensemble:
         self.step_async(n)
         return self.sync()
 
+    def set_stream(self, stream_handle: int | None):
+        st = self.lib.mhd3d_ensemble_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None)
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_set_stream")
+
     def tune(self, steps: int = 3) -> dict:
         z, c, ms = C.c_int32(), C.c_int32(), C.c_double()
         st = self.lib.mhd3d_ensemble_tune(self.h, steps, C.byref(z), C.byref(c), C.byref(ms))
         if st:
             raise Mhd3dError(st, "mhd3d_ensemble_tune")
         return {"zlen": z.value, "ctas_per_sm": c.value, "ms_per_step": ms.value}
+
+
+def par1_record(cfg: RunConfig, ncase=1, ncasep=1, ntotal=1000, nstep0=100, nstart=0, npe=1, npey=1, nit=0,
+                dt=0.0, par64=0.0, par65=0.0) -> np.ndarray:
+    """The reference's 96-value PAR1 dump record (mhd3d_host_par1)."""
+    out = np.zeros(96)
+    ip = np.array([ncase, ncasep, ntotal, nstep0, nstart], dtype=np.int32)
+    host_lib().mhd3d_host_par1(C.byref(cfg), ip.ctypes.data_as(C.c_void_p), npe, npey, nit, dt, par64, par65,
+                               out.ctypes.data_as(C.c_void_p))
+    return out
+
+
+def write_dump(fout: str, ndump: int, par1: np.ndarray, cfg: RunConfig, state: dict, timt: float, timc: float,
+               umach: float, dt: float):
+    """Dump ndump of a single-domain state in the reference's .dat0/.par/.lis layout."""
+    st = host_lib().mhd3d_host_write_dump(fout.encode(), ndump, np.ascontiguousarray(par1).ctypes.data_as(C.c_void_p),
+                                          cfg.npx, cfg.npy, cfg.npz, cfg.lmag,
+                                          *[_ptr(None if state.get(f) is None else np.asfortranarray(state[f]))
+                                            for f in FIELDS], timt, timc, umach, dt)
+    if st:
+        raise Mhd3dError(st, "mhd3d_host_write_dump")
+
+
+def read_dump(finp: str, nstart: int, npey: int, npez: int, cfg: RunConfig):
+    """Restart state from dump nstart (1-based) of a run with npey x npez ranks."""
+    shape = (cfg.npx + 2, cfg.npy + 2, cfg.npz + 2)
+    out = {f: np.zeros(shape, order="F") for f in FIELDS[:5]}
+    for f in FIELDS[5:]:
+        out[f] = np.zeros(shape, order="F") if cfg.lmag else None
+    par1 = np.zeros(96)
+    st = host_lib().mhd3d_host_read_dump(finp.encode(), nstart, npey, npez, cfg.lmag, cfg.npx, cfg.npy, cfg.npz,
+                                         par1.ctypes.data_as(C.c_void_p), *[_ptr(out[f]) for f in FIELDS])
+    if st:
+        raise Mhd3dError(st, "mhd3d_host_read_dump")
+    return out, par1
