@@ -276,6 +276,29 @@ int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_p
 /* enqueue the ensemble's work on a caller's cudaStream_t (NULL: its own) */
 int mhd3d_ensemble_set_stream(void* ens, void* stream);
 
+/*
+ * Learned-closure building blocks (no counterpart in the reference).  All
+ * arrays are device pointers; activations are channels-last BF16
+ * [nz][ny][nx][C] (periodic in x and y, zero outside in z), weights BF16
+ * [cout][27*cin] with k = tap*cin + ci, tap = (dx+1) + 3*(dy+1) + 9*(dz+1).
+ * nx must be a multiple of 128.  Supported (cin, cout): (16,32), (32,32),
+ * (32,16).  Work is enqueued on stream; err (device int) is set non-zero if
+ * a bounded wait of the tensor-core pipeline gave up.
+ *
+ * mhd3d_conv3d: y = act(conv(x, w) + bias), act = ReLU if relu; with mask
+ * (channels-last, cout channels) the output is zeroed where mask <= 0 (the
+ * ReLU derivative in the input-gradient pass).  y (BF16) and/or yf (FP32).
+ * mhd3d_conv3d_wtranspose: w -> wt, the weights of the input-gradient
+ * convolution (cin and cout swapped, taps mirrored).
+ * mhd3d_conv3d_wgrad: dw[cout][27*cin] += sum over voxels of dy (x) x
+ * shifted, db[cout] += sum of dy (FP32, accumulating).
+ */
+int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const float* bias, const void* mask,
+                 int32_t relu, void* y, float* yf, int32_t nx, int32_t ny, int32_t nz, int32_t* err, void* stream);
+int mhd3d_conv3d_wtranspose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
+int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, float* db, int32_t nx,
+                       int32_t ny, int32_t nz, void* stream);
+
 const char* mhd3d_version(void);
 
 #ifdef __cplusplus

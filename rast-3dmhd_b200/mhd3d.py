@@ -119,6 +119,10 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_ensemble_step.argtypes = [vp, C.c_int32]
     lib.mhd3d_ensemble_sync.argtypes = [vp, vp, vp, vp, vp]
     lib.mhd3d_ensemble_set_stream.argtypes = [vp, vp]
+    i32 = C.c_int32
+    lib.mhd3d_conv3d.argtypes = [i32, i32, vp, vp, vp, vp, i32, vp, vp, i32, i32, i32, vp, vp]
+    lib.mhd3d_conv3d_wtranspose.argtypes = [i32, i32, vp, vp, vp]
+    lib.mhd3d_conv3d_wgrad.argtypes = [i32, i32, vp, vp, vp, vp, i32, i32, i32, vp]
     lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_double)]
     lib.mhd3d_version.restype = C.c_char_p
