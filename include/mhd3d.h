@@ -123,7 +123,8 @@ int mhd3d_destroy(void* handle);
  * of the reference's dump records RU,RV,RW,TT,RO[,BX,BY,BZ]
  * (3dmhd.f:941-962).  bx/by/bz may be NULL when lmag == 0.  The x/y halos
  * of the uploaded arrays are ignored (the library wraps periodically); the
- * z ghost planes K=1 and K=NZ are kept, as the reference keeps them.
+ * z ghost planes K=1 and K=NZ are kept, as the reference keeps them.  The
+ * arrays may be host or device memory (mhd3d_download likewise).
  */
 int mhd3d_upload(void* handle,
                  const double* ru, const double* rv, const double* rw,
@@ -298,6 +299,42 @@ int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const 
 int mhd3d_conv3d_wtranspose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
 int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, float* db, int32_t nx,
                        int32_t ny, int32_t nz, void* stream);
+
+/*
+ * Learned closure on an FP32 handle whose NPX is a multiple of 128.
+ * mhd3d_closure_set attaches a trained network (weights BF16 [cout][27*cin]:
+ * w1 32x432, w2 32x864, w3 16x864; biases FP32 32, 32, 16; in_scale[8] the
+ * feature scales; out_scale[12] the target scales; host or device pointers,
+ * copied): every step then evaluates it once before stage 1 and adds its
+ * tendencies (RU_i -= d_j tau_ij, TT -= (1/RO) d_j q_j, B += curl eps) to the
+ * three stages.  When an output is not finite, or the stress trace exceeds
+ * trip x RO*TT, that step runs without it (the plain coarse method).  A
+ * NULL w1 detaches.  mhd3d_closure_status: steps that fell back, evaluations,
+ * and the tensor-core pipeline's error flag.
+ *
+ * Training support (device pointers, enqueued on stream):
+ * mhd3d_coarsen: box filter of a handle's state by fac: coarse state in
+ * Fortran (NX,NY,NZ) arrays (8 or 5 fields, halos periodic, ghost planes =
+ * walls) and the subgrid targets [k][j][i][12] (tau_xx,yy,zz,xy,xz,yz, q_x,y,z,
+ * eps_x,y,z).  mhd3d_closure_features: network input [k][j][i][16] BF16 of a
+ * handle's state (u, v, w, TT-<TT>, RO-<RO>, BX, BY-<BY>, BZ times in_scale;
+ * means: 3*NPZ doubles of scratch).  mhd3d_closure_loss: adds the mean-square
+ * error of pred [v][16] against target [v][12] to *loss and writes its
+ * gradient dy [v][16] BF16.  mhd3d_adam: one Adam step on FP32 parameters
+ * (step number t), optional BF16 copy.  mhd3d_closure_tendency: the
+ * tendencies of pred for a handle's state, out[f][k][j][i] (f = RU, RV, RW,
+ * TT, BX, BY, BZ); *flag set when the indicator trips.
+ */
+int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void* w2, const float* b2, const void* w3,
+                      const float* b3, const float* in_scale, const float* out_scale, float trip);
+int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* err);
+int mhd3d_coarsen(void* fine, int32_t fac, double* cstate, float* targets, void* stream);
+int mhd3d_closure_features(void* handle, const float* in_scale, void* feat, double* means, void* stream);
+int mhd3d_closure_loss(const float* pred, const float* target, int64_t nvox, void* dy, double* loss, void* stream);
+int mhd3d_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+               int32_t t, void* p_bf16, void* stream);
+int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_scale, float* out, int32_t* flag,
+                           float trip, void* stream);
 
 const char* mhd3d_version(void);
 

@@ -1,6 +1,7 @@
 // mhd3d_api.cu -- the C-ABI of include/mhd3d.h: handle life cycle, layout
 // conversion between the reference's Fortran arrays and the device layout,
 // and the step loop with its device-side bookkeeping.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +48,16 @@ struct Handle {
     std::vector<double> faz_h, fbz_h, fcz_h;   // host copies of the z stencil factors
     std::vector<double> rka_h, dka_h, ddz_h;   // and of RKAPA, DKAPA, DDZ
     ColC* cxy = nullptr;                       // FP32 column constants: NX in x, then NY in y
+    // learned closure attached to an FP32 handle (mhd3d_closure_set)
+    bool clo = false;
+    void* cbuf = nullptr;                      // one allocation for everything below
+    __nv_bfloat16 *cw[3] = {nullptr, nullptr, nullptr};
+    float *cb[3] = {nullptr, nullptr, nullptr}, *cin_scale = nullptr, *cout_scale = nullptr;
+    __nv_bfloat16 *cfeat = nullptr, *cact1 = nullptr, *cact2 = nullptr;
+    float *cpred = nullptr, *cfcl = nullptr;
+    double* cmeans = nullptr;                  // 3 x NPZ horizontal means (T, RO, BY)
+    int* cflag = nullptr;                      // [0] trip flag of the current evaluation, [1] trips, [2] evaluations, [3] kernel error
+    float ctrip = 1.f;
     Scalars32 s32{};
     double top_lin = 0.0, top_tb = 0.0;
     float t_top_fix = 0.f, t_top_fix4 = 0.f, t_top_flux = 0.f, t_bot = 0.f;
@@ -293,6 +304,260 @@ __global__ void k_reset(Control* ctl, Accum* acc, int clear_stop, unsigned long 
 // End of a step (advance=1: NIT, TIMC, TIMT of STEP 3dmhdsub.f:1171-1173 and
 // the driver's DT check 3dmhd.f:924) and DT/UMACH of the next step from the
 // CFL accumulators (DT=SF*MIN(...), 3dmhdsub.f:866-873; UMACH=SQRT(...), 761).
+// ---- learned closure (no counterpart in the reference) ----------------------
+// Reads of a handle's state as full FP64 values, for either precision.
+struct UView {
+    const void* u;        // U buffer (double, or float perturbations)
+    const double* bgd;    // FP32 form: backgrounds (5 x NZ), else null
+    size_t uf, uz, NZ;
+    int upitch, f32;
+};
+__device__ __forceinline__ double uget(const UView& v, int f, int i, int j, int K)
+{
+    // i, j, K: U-layout indices (halo / ghost plane at 0)
+    const size_t off = (size_t)f * v.uf + (size_t)K * v.uz + (size_t)j * v.upitch + i;
+    if (v.f32) {
+        const double x = (double)static_cast<const float*>(v.u)[off];
+        const int bi = f == F_RO ? 0 : f == F_TT ? 1 : f == F_BX ? 2 : f == F_BY ? 3 : f == F_BZ ? 4 : -1;
+        return bi >= 0 ? v.bgd[bi * v.NZ + K] + x : x;
+    }
+    return static_cast<const double*>(v.u)[off];
+}
+
+// Box filter by fac in every direction (interior cells fac*i..fac*i+fac-1) of a
+// fine state: the coarse state (Favre temperature TT = <RO*TT>/<RO>) in
+// Fortran (NXc,NYc,NZc) arrays, and the subgrid targets channels-last
+// [k][j][i][12]: tau_xx,yy,zz,xy,xz,yz = <RO u_i u_j> - <RU_i><RU_j>/<RO>,
+// q_x,y,z = <RU_i TT> - <RU_i><RO TT>/<RO>, eps = <u x B> - (<RU>/<RO>) x <B>.
+__global__ void k_coarsen(UView fine, int fac, int npxc, int npyc, int npzc, int lmag, double* __restrict__ cs,
+                          float* __restrict__ tg)
+{
+    const size_t n = (size_t)npxc * npyc * npzc;
+    const size_t NXc = npxc + 2, NYc = npyc + 2, NC = NXc * NYc * (npzc + 2);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int ic = (int)(q % npxc), jc = (int)((q / npxc) % npyc), kc = (int)(q / ((size_t)npxc * npyc));
+        double R = 0, M[3] = {0, 0, 0}, E = 0, B[3] = {0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0}, H[3] = {0, 0, 0};
+        double X[3] = {0, 0, 0};
+        for (int c = 0; c < fac; ++c)
+            for (int b = 0; b < fac; ++b)
+                for (int a = 0; a < fac; ++a) {
+                    const int i = fac * ic + a + 1, j = fac * jc + b + 1, K = fac * kc + c + 1;
+                    const double ro = uget(fine, F_RO, i, j, K), tt = uget(fine, F_TT, i, j, K);
+                    const double m0 = uget(fine, F_RU, i, j, K), m1 = uget(fine, F_RV, i, j, K),
+                                 m2 = uget(fine, F_RW, i, j, K);
+                    const double ri = 1.0 / ro, u0 = m0 * ri, u1 = m1 * ri, u2 = m2 * ri;
+                    R += ro;
+                    M[0] += m0; M[1] += m1; M[2] += m2;
+                    E += ro * tt;
+                    S[0] += m0 * u0; S[1] += m1 * u1; S[2] += m2 * u2;
+                    S[3] += m0 * u1; S[4] += m0 * u2; S[5] += m1 * u2;
+                    H[0] += m0 * tt; H[1] += m1 * tt; H[2] += m2 * tt;
+                    if (lmag) {
+                        const double bx = uget(fine, F_BX, i, j, K), by = uget(fine, F_BY, i, j, K),
+                                     bz = uget(fine, F_BZ, i, j, K);
+                        B[0] += bx; B[1] += by; B[2] += bz;
+                        X[0] += u1 * bz - u2 * by;
+                        X[1] += u2 * bx - u0 * bz;
+                        X[2] += u0 * by - u1 * bx;
+                    }
+                }
+        const double w = 1.0 / ((double)fac * fac * fac);
+        R *= w; E *= w;
+        for (int t = 0; t < 3; ++t) { M[t] *= w; B[t] *= w; H[t] *= w; X[t] *= w; }
+        for (int t = 0; t < 6; ++t) S[t] *= w;
+        const size_t fo = (size_t)(ic + 1) + NXc * ((size_t)(jc + 1) + NYc * (size_t)(kc + 1));
+        cs[F_RU * NC + fo] = M[0];
+        cs[F_RV * NC + fo] = M[1];
+        cs[F_RW * NC + fo] = M[2];
+        cs[F_TT * NC + fo] = E / R;
+        cs[F_RO * NC + fo] = R;
+        if (lmag) {
+            cs[F_BX * NC + fo] = B[0];
+            cs[F_BY * NC + fo] = B[1];
+            cs[F_BZ * NC + fo] = B[2];
+        }
+        const double ri = 1.0 / R, v0 = M[0] * ri, v1 = M[1] * ri, v2 = M[2] * ri;
+        float* o = tg + q * 12;
+        o[0] = (float)(S[0] - M[0] * v0);
+        o[1] = (float)(S[1] - M[1] * v1);
+        o[2] = (float)(S[2] - M[2] * v2);
+        o[3] = (float)(S[3] - M[0] * v1);
+        o[4] = (float)(S[4] - M[0] * v2);
+        o[5] = (float)(S[5] - M[1] * v2);
+        o[6] = (float)(H[0] - M[0] * E * ri);
+        o[7] = (float)(H[1] - M[1] * E * ri);
+        o[8] = (float)(H[2] - M[2] * E * ri);
+        o[9] = (float)(X[0] - (v1 * B[2] - v2 * B[1]));
+        o[10] = (float)(X[1] - (v2 * B[0] - v0 * B[2]));
+        o[11] = (float)(X[2] - (v0 * B[1] - v1 * B[0]));
+    }
+}
+
+// Fortran (NX,NY,NZ) arrays: periodic halos from the interior, z ghost planes = wall planes
+__global__ void k_fort_wrap(double* __restrict__ a, int nf, int npx, int npy, int npz)
+{
+    const size_t NX = npx + 2, NY = npy + 2, NZ = npz + 2, NC = NX * NY * NZ;
+    const size_t n = (size_t)nf * NC;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t f = q / NC, r = q % NC;
+        const int I = (int)(r % NX), J = (int)((r / NX) % NY), K = (int)(r / (NX * NY));
+        const bool halo = I == 0 || I == (int)NX - 1 || J == 0 || J == (int)NY - 1 || K == 0 || K == (int)NZ - 1;
+        if (!halo) continue;
+        const int Is = I == 0 ? npx : (I == (int)NX - 1 ? 1 : I);
+        const int Js = J == 0 ? npy : (J == (int)NY - 1 ? 1 : J);
+        const int Ks = K == 0 ? 1 : (K == (int)NZ - 1 ? npz : K);
+        a[q] = a[f * NC + (size_t)Is + NX * ((size_t)Js + NY * (size_t)Ks)];
+    }
+}
+
+// per-plane horizontal means of TT, RO, BY (network features)
+__global__ void __launch_bounds__(256) k_hmeans3(UView v, int npx, int npy, double* __restrict__ means, int npz,
+                                                 int lmag)
+{
+    __shared__ double red[256];
+    const int k = blockIdx.x;
+    double st = 0, sr = 0, sb = 0;
+    for (int q = threadIdx.x; q < npx * npy; q += 256) {
+        const int i = q % npx + 1, j = q / npx + 1;
+        st += uget(v, F_TT, i, j, k + 1);
+        sr += uget(v, F_RO, i, j, k + 1);
+        if (lmag) sb += uget(v, F_BY, i, j, k + 1);
+    }
+    double* outs[3] = {&st, &sr, &sb};
+    for (int t = 0; t < 3; ++t) {
+        red[threadIdx.x] = *outs[t];
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) means[t * npz + k] = red[0] / ((double)npx * npy);
+        __syncthreads();
+    }
+}
+
+// network input, channels-last BF16 [k][j][i][16]: u, v, w, TT-<TT>, RO-<RO>, BX, BY-<BY>, BZ
+// times in_scale, channels 8..15 zero
+__global__ void k_features(UView v, const double* __restrict__ means, const float* __restrict__ sc, int npx, int npy,
+                           int npz, int lmag, __nv_bfloat16* __restrict__ feat)
+{
+    const size_t n = (size_t)npx * npy * npz;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % npx) + 1, j = (int)((q / npx) % npy) + 1, k = (int)(q / ((size_t)npx * npy));
+        const double ro = uget(v, F_RO, i, j, k + 1), ri = 1.0 / ro;
+        float f[8];
+        f[0] = (float)(uget(v, F_RU, i, j, k + 1) * ri);
+        f[1] = (float)(uget(v, F_RV, i, j, k + 1) * ri);
+        f[2] = (float)(uget(v, F_RW, i, j, k + 1) * ri);
+        f[3] = (float)(uget(v, F_TT, i, j, k + 1) - means[k]);
+        f[4] = (float)(ro - means[npz + k]);
+        f[5] = lmag ? (float)uget(v, F_BX, i, j, k + 1) : 0.f;
+        f[6] = lmag ? (float)(uget(v, F_BY, i, j, k + 1) - means[2 * npz + k]) : 0.f;
+        f[7] = lmag ? (float)uget(v, F_BZ, i, j, k + 1) : 0.f;
+        __align__(16) __nv_bfloat16 h[16];
+        for (int c = 0; c < 8; ++c) h[c] = __float2bfloat16_rn(f[c] * sc[c]);
+        for (int c = 8; c < 16; ++c) h[c] = __float2bfloat16_rn(0.f);
+        uint4* o = reinterpret_cast<uint4*>(feat + q * 16);
+        o[0] = reinterpret_cast<const uint4*>(h)[0];
+        o[1] = reinterpret_cast<const uint4*>(h)[1];
+    }
+}
+
+// mean-square error over 12 channels and its gradient (BF16, channels 12..15 zero)
+__global__ void __launch_bounds__(256) k_closure_loss(const float* __restrict__ pred, const float* __restrict__ tgt,
+                                                      size_t nvox, __nv_bfloat16* __restrict__ dy,
+                                                      double* __restrict__ loss)
+{
+    __shared__ double red[256];
+    const double nrm = 1.0 / ((double)nvox * 12.0);
+    double acc = 0.0;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nvox; q += (size_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < 16; ++c) {
+            float g = 0.f;
+            if (c < 12) {
+                const double d = (double)pred[q * 16 + c] - (double)tgt[q * 12 + c];
+                acc += d * d * nrm;
+                g = (float)(2.0 * d * nrm);
+            }
+            if (dy) dy[q * 16 + c] = __float2bfloat16_rn(g);
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, red[0]);
+}
+
+// Adam on FP32 master parameters; optional BF16 copy
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float bc1, float bc2,
+                       __nv_bfloat16* __restrict__ pb)
+{
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.f - b1) * gq;
+        const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        const float pq = p[q] - lr * (mq / bc1) / (sqrtf(vq / bc2) + eps);
+        p[q] = pq;
+        if (pb) pb[q] = __float2bfloat16_rn(pq);
+    }
+}
+
+// Closure tendencies from the network output (normalised targets x out_scale):
+// RU_i -= d_j tau_ij, TT -= (1/RO) d_j q_j, B += curl eps, centred differences
+// with the grid's metric factors (HX*DXXDX ...), zero on the wall planes.
+// Output field f (RU,RV,RW,TT,BX,BY,BZ) at out[f*fstride + k*kstride + j*jstride + i].
+// flag[0] is set when an output is not finite or the stress exceeds trip x RO*TT.
+__global__ void k_tendency(UView v, const float* __restrict__ pred, const float* __restrict__ osc,
+                           const double* __restrict__ fax, const double* __restrict__ fay,
+                           const double* __restrict__ faz, int npx, int npy, int npz, float trip,
+                           float* __restrict__ out, size_t fstride, size_t kstride, size_t jstride, int* flag)
+{
+    const size_t n = (size_t)npx * npy * npz;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % npx), j = (int)((q / npx) % npy), k = (int)(q / ((size_t)npx * npy));
+        float* o = out + (size_t)k * kstride + (size_t)j * jstride + i;
+        const float* pc = pred + q * 16;
+        bool bad = false;
+        for (int c = 0; c < 12; ++c) bad |= !isfinite(pc[c]);
+        const double ro = uget(v, F_RO, i + 1, j + 1, k + 1), tt = uget(v, F_TT, i + 1, j + 1, k + 1);
+        const double tr = (fabs((double)pc[0] * osc[0]) + fabs((double)pc[1] * osc[1]) + fabs((double)pc[2] * osc[2]));
+        if (bad || !(tr <= (double)trip * ro * tt)) atomicOr(flag, 1);
+        if (k == 0 || k == npz - 1) {
+            for (int f = 0; f < 7; ++f) o[f * fstride] = 0.f;
+            continue;
+        }
+        const int ip = i + 1 == npx ? 0 : i + 1, im = i == 0 ? npx - 1 : i - 1;
+        const int jp = j + 1 == npy ? 0 : j + 1, jm = j == 0 ? npy - 1 : j - 1;
+        auto P = [&](int ii, int jj, int kk, int c) -> double {
+            return (double)pred[(((size_t)kk * npy + jj) * npx + ii) * 16 + c] * osc[c];
+        };
+        const double ax = fax[i + 1], ay = fay[j + 1], az = faz[k + 1];
+        auto dx = [&](int c) { return (P(ip, j, k, c) - P(im, j, k, c)) * ax; };
+        auto dy = [&](int c) { return (P(i, jp, k, c) - P(i, jm, k, c)) * ay; };
+        auto dz = [&](int c) { return (P(i, j, k + 1, c) - P(i, j, k - 1, c)) * az; };
+        o[0 * fstride] = (float)(-(dx(0) + dy(3) + dz(4)));
+        o[1 * fstride] = (float)(-(dx(3) + dy(1) + dz(5)));
+        o[2 * fstride] = (float)(-(dx(4) + dy(5) + dz(2)));
+        o[3 * fstride] = (float)(-(dx(6) + dy(7) + dz(8)) / ro);
+        o[4 * fstride] = (float)(dy(11) - dz(10));
+        o[5 * fstride] = (float)(dz(9) - dx(11));
+        o[6 * fstride] = (float)(dx(10) - dy(9));
+    }
+}
+
+__global__ void k_trip_count(int* flag)
+{
+    flag[1] += flag[0] ? 1 : 0;
+    flag[2] += 1;
+}
+
+
 __device__ void finalize_one(Control* ctl, Accum* acc, double sf, double dtmin, int lmag, int advance,
                              unsigned long long w4key)
 {
@@ -397,6 +662,8 @@ StageArgs32 make_args32(Handle* h)
     a.cx = h->cxy;
     a.cy = h->cxy + (h->p.npx + 2);
     a.s32 = h->s32;
+    a.fcl = h->clo ? h->cfcl : nullptr;
+    a.fcl_flag = h->cflag;
     a.top_lin = h->top_lin;
     a.top_tb = h->top_tb;
     a.t_top_fix = h->t_top_fix;
@@ -480,6 +747,7 @@ int destroy(Handle* h)
     cudaFree(h->bg32);
     cudaFree(h->pb);
     cudaFree(h->cxy);
+    cudaFree(h->cbuf);
     cudaFree(h->ctl);
     cudaFree(h->acc);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -851,7 +1119,7 @@ int upload(Handle* h, const double* const f[8])
     for (int i = 0; i < h->nf; ++i)
         if (!f[i]) return MHD3D_ERR_ARG;
     for (int fi = 0; fi < h->nf; ++fi) {
-        CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyDefault, h->st));
         if (h->f32) {
             const int bi = bg_index(fi);
             double* bg = bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr;
@@ -894,7 +1162,7 @@ int download(Handle* h, double* const f[8])
                                                        npz, h->upitch, h->uz);
         }
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDefault, h->st));
     }
     CK(cudaStreamSynchronize(h->st));
     return MHD3D_OK;
@@ -926,6 +1194,8 @@ int record_event(Handle* h, int stage)
     return MHD3D_OK;
 }
 
+int closure_eval(Handle* h, int cur);
+
 int step_async(Handle* h, int n)
 {
     CK(cudaSetDevice(h->dev));
@@ -942,6 +1212,10 @@ int step_async(Handle* h, int n)
     }
     int cur = h->cur_base ^ (h->pending & 1);
     for (int s = 0; s < n; ++s) {
+        if (h->clo) {
+            int st = closure_eval(h, cur);
+            if (st) return st;
+        }
         for (int stg = 1; stg <= 3; ++stg) {
             if (h->prof) {
                 int st = record_event(h, stg - 1);
@@ -1048,6 +1322,93 @@ int profiles(Handle* h, double* out)
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, dout, sizeof(double) * MHD3D_NPROF * npz, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
+UView uview(const Handle* h, int cur)
+{
+    UView v;
+    v.u = h->ubuf[cur];
+    v.bgd = h->f32 ? h->bgd : nullptr;
+    v.uf = h->uf;
+    v.uz = h->uz;
+    v.NZ = (size_t)h->p.npz + 2;
+    v.upitch = h->upitch;
+    v.f32 = h->f32 ? 1 : 0;
+    return v;
+}
+
+// one evaluation of the attached closure on buffer cur: features, three
+// convolutions, tendencies and the error indicator, all on the handle's stream
+int closure_eval(Handle* h, int cur)
+{
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nv = (size_t)npx * npy * npz;
+    const UView v = uview(h, cur);
+    CK(cudaMemsetAsync(h->cflag, 0, sizeof(int), h->st));
+    k_hmeans3<<<npz, 256, 0, h->st>>>(v, npx, npy, h->cmeans, npz, h->p.lmag);
+    k_features<<<grid_for(nv), 256, 0, h->st>>>(v, h->cmeans, h->cin_scale, npx, npy, npz, h->p.lmag, h->cfeat);
+    CK(cudaGetLastError());
+    int32_t* err = h->cflag + 3;
+    if (mhd3d_conv3d(16, 32, h->cfeat, h->cw[0], h->cb[0], nullptr, 1, h->cact1, nullptr, npx, npy, npz, err, h->st) ||
+        mhd3d_conv3d(32, 32, h->cact1, h->cw[1], h->cb[1], nullptr, 1, h->cact2, nullptr, npx, npy, npz, err, h->st) ||
+        mhd3d_conv3d(32, 16, h->cact2, h->cw[2], h->cb[2], nullptr, 0, nullptr, h->cpred, npx, npy, npz, err, h->st))
+        return MHD3D_ERR_CUDA;
+    k_tendency<<<grid_for(nv), 256, 0, h->st>>>(v, h->cpred, h->cout_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy,
+                                                npz, h->ctrip, h->cfcl, h->zf, h->zz, (size_t)h->zpitch, h->cflag);
+    k_trip_count<<<1, 1, 0, h->st>>>(h->cflag);
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int closure_set(Handle* h, const void* const w[3], const float* const b[3], const float* in_scale,
+                const float* out_scale, float trip)
+{
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    if (!w[0]) {
+        h->clo = false;
+        return MHD3D_OK;
+    }
+    if (!h->f32 || h->p.npx % 128 || !w[1] || !w[2] || !b[0] || !b[1] || !b[2] || !in_scale || !out_scale)
+        return MHD3D_ERR_ARG;
+    const size_t nv = (size_t)h->p.npx * h->p.npy * h->p.npz;
+    const size_t wn[3] = {32 * 27 * 16, 32 * 27 * 32, 16 * 27 * 32}, bn[3] = {32, 32, 16};
+    if (!h->cbuf) {
+        size_t bytes = 0;
+        auto take = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) / 256 * 256; return o; };
+        size_t ow[3], ob[3];
+        for (int l = 0; l < 3; ++l) ow[l] = take(wn[l] * 2), ob[l] = take(bn[l] * 4);
+        const size_t oin = take(8 * 4), oout = take(12 * 4), ofeat = take(nv * 16 * 2), oa1 = take(nv * 32 * 2),
+                     oa2 = take(nv * 32 * 2), opred = take(nv * 16 * 4), ofcl = take((size_t)7 * h->zf * 4),
+                     omeans = take((size_t)3 * h->p.npz * 8), oflag = take(4 * 4);
+        CK(cudaMalloc(&h->cbuf, bytes));
+        CK(cudaMemset(h->cbuf, 0, bytes));
+        char* base = static_cast<char*>(h->cbuf);
+        for (int l = 0; l < 3; ++l) {
+            h->cw[l] = reinterpret_cast<__nv_bfloat16*>(base + ow[l]);
+            h->cb[l] = reinterpret_cast<float*>(base + ob[l]);
+        }
+        h->cin_scale = reinterpret_cast<float*>(base + oin);
+        h->cout_scale = reinterpret_cast<float*>(base + oout);
+        h->cfeat = reinterpret_cast<__nv_bfloat16*>(base + ofeat);
+        h->cact1 = reinterpret_cast<__nv_bfloat16*>(base + oa1);
+        h->cact2 = reinterpret_cast<__nv_bfloat16*>(base + oa2);
+        h->cpred = reinterpret_cast<float*>(base + opred);
+        h->cfcl = reinterpret_cast<float*>(base + ofcl);
+        h->cmeans = reinterpret_cast<double*>(base + omeans);
+        h->cflag = reinterpret_cast<int*>(base + oflag);
+    }
+    for (int l = 0; l < 3; ++l) {
+        CK(cudaMemcpyAsync(h->cw[l], w[l], wn[l] * 2, cudaMemcpyDefault, h->st));
+        CK(cudaMemcpyAsync(h->cb[l], b[l], bn[l] * 4, cudaMemcpyDefault, h->st));
+    }
+    CK(cudaMemcpyAsync(h->cin_scale, in_scale, 8 * 4, cudaMemcpyDefault, h->st));
+    CK(cudaMemcpyAsync(h->cout_scale, out_scale, 12 * 4, cudaMemcpyDefault, h->st));
+    CK(cudaMemsetAsync(h->cflag, 0, 4 * sizeof(int), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->ctrip = trip;
+    h->clo = true;
     return MHD3D_OK;
 }
 
@@ -1501,6 +1862,102 @@ int mhd3d_bcon(void* handle)
     CK(h->p.mode == MHD3D_MODE_FAST ? fast::launch_bcon(a, h->st) : exact::launch_bcon(a, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->dt_valid = false;
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void* w2, const float* b2, const void* w3,
+                      const float* b3, const float* in_scale, const float* out_scale, float trip)
+{
+    if (!handle) return MHD3D_ERR_ARG;
+    const void* w[3] = {w1, w2, w3};
+    const float* b[3] = {b1, b2, b3};
+    return closure_set(static_cast<Handle*>(handle), w, b, in_scale, out_scale, trip);
+}
+
+int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* err)
+{
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h) return MHD3D_ERR_ARG;
+    int f[4] = {0, 0, 0, 0};
+    CK(cudaSetDevice(h->dev));
+    if (h->cflag) {
+        CK(cudaMemcpyAsync(f, h->cflag, sizeof f, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
+    if (trips) *trips = f[1];
+    if (evals) *evals = f[2];
+    if (err) *err = f[3];
+    return MHD3D_OK;
+}
+
+int mhd3d_coarsen(void* fine, int32_t fac, double* cstate, float* targets, void* stream)
+{
+    Handle* h = static_cast<Handle*>(fine);
+    if (!h || fac < 1 || !cstate || !targets || h->p.npx % fac || h->p.npy % fac || h->p.npz % fac) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    CK(cudaStreamSynchronize(h->st));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int npxc = h->p.npx / fac, npyc = h->p.npy / fac, npzc = h->p.npz / fac;
+    const size_t nc = (size_t)npxc * npyc * npzc;
+    k_coarsen<<<grid_for(nc), 128, 0, s>>>(uview(h, h->cur), fac, npxc, npyc, npzc, h->p.lmag, cstate, targets);
+    const size_t nfull = (size_t)(h->p.lmag ? 8 : 5) * (npxc + 2) * (npyc + 2) * (npzc + 2);
+    k_fort_wrap<<<grid_for(nfull), 256, 0, s>>>(cstate, h->p.lmag ? 8 : 5, npxc, npyc, npzc);
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_features(void* handle, const float* in_scale, void* feat, double* means, void* stream)
+{
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !in_scale || !feat || !means) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    CK(cudaStreamSynchronize(h->st));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const UView v = uview(h, h->cur);
+    k_hmeans3<<<npz, 256, 0, s>>>(v, npx, npy, means, npz, h->p.lmag);
+    k_features<<<grid_for((size_t)npx * npy * npz), 256, 0, s>>>(v, means, in_scale, npx, npy, npz, h->p.lmag,
+                                                                static_cast<__nv_bfloat16*>(feat));
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_loss(const float* pred, const float* target, int64_t nvox, void* dy, double* loss, void* stream)
+{
+    if (!pred || !target || nvox <= 0 || !loss) return MHD3D_ERR_ARG;
+    k_closure_loss<<<grid_for((size_t)nvox), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        pred, target, (size_t)nvox, static_cast<__nv_bfloat16*>(dy), loss);
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+               int32_t t, void* p_bf16, void* stream)
+{
+    if (!p || !g || !m || !v || n <= 0 || t < 1) return MHD3D_ERR_ARG;
+    const float bc1 = 1.f - powf(b1, (float)t), bc2 = 1.f - powf(b2, (float)t);
+    k_adam<<<grid_for((size_t)n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        p, g, m, v, (size_t)n, lr, b1, b2, eps, bc1, bc2, static_cast<__nv_bfloat16*>(p_bf16));
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_scale, float* out, int32_t* flag,
+                           float trip, void* stream)
+{
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !pred || !out_scale || !out || !flag) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    CK(cudaStreamSynchronize(h->st));
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nv = (size_t)npx * npy * npz;
+    k_tendency<<<grid_for(nv), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        uview(h, h->cur), pred, out_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy, npz, trip, out, nv,
+        (size_t)npx * npy, (size_t)npx, flag);
+    CK(cudaGetLastError());
     return MHD3D_OK;
 }
 

@@ -175,6 +175,8 @@ struct StageArgs32 {
     const ColC* cx;           // per x column (Fortran I=1..NX)
     const ColC* cy;           // per y row (Fortran J=1..NY)
     Scalars32 s32;
+    const float* fcl;         // learned-closure tendencies (RU,RV,RW,TT,BX,BY,BZ in the Z layout) or null
+    const int* fcl_flag;      // non-zero: the closure's error indicator tripped for this step
     double top_lin, top_tb;   // C43*Tb(3)-C13*Tb(4)-Tb(2) and Tb(2): top-wall temperature in perturbation form
     float t_top_fix, t_top_fix4, t_top_flux, t_bot;   // wall T' constants (ITC 0/2/4, ITC=4 left half, ITC=1; IZC)
     size_t uf, uz, zf, zz;

@@ -192,6 +192,7 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
     const size_t ucol = (size_t)(gj + 1) * a.upitch + (gi + 1);
     const size_t zcol = (size_t)gj * a.zpitch + gi;
     const HaloCols hc = halo_cols(npx, npy, a.upitch, gi, gj);
+    const bool use_fcl = STAGE != 0 && a.fcl != nullptr && *a.fcl_flag == 0;
 
     // the stop flag is read once, by one thread, so the CTA takes one path
     if (tid == 0) {
@@ -443,6 +444,19 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
                     a.f_out[zc + 7 * a.zf] = wall ? 0.f : w3;
                 }
             } else {
+                // learned closure: its tendencies, fixed over the step, join the right-hand side
+                if (use_fcl) {
+                    const float* fc = a.fcl + zc;
+                    fu += fc[0];
+                    fv += fc[a.zf];
+                    fw += fc[2 * a.zf];
+                    ft += fc[3 * a.zf];
+                    if (MAG) {
+                        w1 += fc[4 * a.zf];
+                        w2 += fc[5 * a.zf];
+                        w3 += fc[6 * a.zf];
+                    }
+                }
                 // RK3 update of the perturbations (the backgrounds do not change)
                 float zu, zv, zw, zr, zt, zbx = 0.f, zby = 0.f, zbz = 0.f;
                 if (STAGE == 1) {

@@ -123,6 +123,13 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_conv3d.argtypes = [i32, i32, vp, vp, vp, vp, i32, vp, vp, i32, i32, i32, vp, vp]
     lib.mhd3d_conv3d_wtranspose.argtypes = [i32, i32, vp, vp, vp]
     lib.mhd3d_conv3d_wgrad.argtypes = [i32, i32, vp, vp, vp, vp, i32, i32, i32, vp]
+    lib.mhd3d_closure_set.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_float]
+    lib.mhd3d_closure_status.argtypes = [vp, vp, vp, vp]
+    lib.mhd3d_coarsen.argtypes = [vp, i32, vp, vp, vp]
+    lib.mhd3d_closure_features.argtypes = [vp, vp, vp, vp, vp]
+    lib.mhd3d_closure_loss.argtypes = [vp, vp, C.c_int64, vp, vp, vp]
+    lib.mhd3d_adam.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, i32, vp, vp]
+    lib.mhd3d_closure_tendency.argtypes = [vp, vp, vp, vp, vp, C.c_float, vp]
     lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_double)]
     lib.mhd3d_version.restype = C.c_char_p
@@ -314,6 +321,13 @@ class GpuSim:
         if st:
             raise Mhd3dError(st, "mhd3d_profiles")
         return out
+
+    def closure_status(self) -> dict:
+        t, e, r = C.c_int32(), C.c_int32(), C.c_int32()
+        st = self.lib.mhd3d_closure_status(self.h, C.byref(t), C.byref(e), C.byref(r))
+        if st:
+            raise Mhd3dError(st, "mhd3d_closure_status")
+        return {"trips": t.value, "evals": e.value, "err": r.value}
 
     def cfl(self):
         dt, um = C.c_double(), C.c_double()
