@@ -183,6 +183,202 @@ def run_reference_arm(args, rank, world):
     return line
 
 
+ENSEMBLE_NAME = ("batched FP32 ensemble: 48 rotating MHD members, grids drawn from {64x64x48, 96x96x64, "
+                 "128x128x96}, Ra log-uniform 1e4-1e6, Ta log-uniform 1e3-1e6, contrast uniform 3-30, "
+                 "perturbation 2e-4, master seed 20261203")
+
+
+def ensemble_setups(mhd3d, seed=20261203, n=48):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    grids = [(64, 64, 48), (96, 96, 64), (128, 128, 96)]
+    out = []
+    for i in range(n):
+        g = grids[rng.integers(3)]
+        ra, ta, con = 10 ** rng.uniform(4, 6), 10 ** rng.uniform(3, 6), rng.uniform(3, 30)
+        cfg = mhd3d.convection_config(*g, ra=ra, ta=ta, contrast=con, ampt=2e-4, seed=i + 1)
+        out.append(mhd3d.make_setup(cfg))
+    return out
+
+
+def run_ensemble(args, rank, world, local):
+    """The batched ensemble: every member's stages in one persistent launch
+    per stage, a step as a CUDA graph, tiles autotuned; value = all members'
+    cells x steps / device time."""
+    import numpy as np
+    import torch
+    import mhd3d
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    setups = ensemble_setups(mhd3d)
+    cells = sum(su.params.npx * su.params.npy * su.params.npz for su in setups)
+    ens = mhd3d.Ensemble(setups)
+    stream = torch.cuda.Stream()
+    ens.set_stream(stream.cuda_stream)
+    for m, su in zip(ens.members, setups):
+        m.upload(su.state)
+    ens.step(1)
+    tuned = ens.tune(steps=3)
+    ens.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local) if rank == 0 else None
+    barrier()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    res = ens.sync()
+    barrier()
+    clk = clocks.stop() if clocks else None
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    peaks, peak_src = measured_peaks()
+    achieved = cells * 320.0 * args.steps / (ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "kernel": "k_stage32_multi (3 persistent launches per step) + k_finalize_multi, whole step",
+            "algorithmic_bytes_per_step": cells * 320.0,
+            "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured" else "fallback 6650 GB/s"}
+    # e2e: upload every member from pinned memory, K steps, download every member
+    pins = []
+    for su in setups:
+        nf = 8
+        sh = su.shape
+        n = sh[0] * sh[1] * sh[2]
+        pin_in = torch.empty((nf, n), dtype=torch.float64, pin_memory=True)
+        pin_out = torch.empty((nf, n), dtype=torch.float64, pin_memory=True)
+        hin = {f: pin_in[i].numpy().reshape(sh, order="F") for i, f in enumerate(mhd3d.FIELDS)}
+        hout = {f: pin_out[i].numpy().reshape(sh, order="F") for i, f in enumerate(mhd3d.FIELDS)}
+        for f in mhd3d.FIELDS:
+            hin[f][...] = su.state[f]
+        pins.append((hin, hout, pin_in, pin_out))
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    wt0 = time.perf_counter()
+    f0.record(stream)
+    for m, (hin, hout, _, _) in zip(ens.members, pins):
+        assert m.lib.mhd3d_upload(m.h, *[mhd3d._ptr(hin[f]) for f in mhd3d.FIELDS]) == 0
+    ens.step_async(args.steps)
+    r2 = ens.sync()
+    for m, (hin, hout, _, _) in zip(ens.members, pins):
+        assert m.lib.mhd3d_download(m.h, *[mhd3d._ptr(hout[f]) for f in mhd3d.FIELDS]) == 0
+    f1.record(stream)
+    f1.synchronize()
+    ms_e2e = max(f0.elapsed_time(f1), (time.perf_counter() - wt0) * 1e3)
+    state_bytes = sum(8 * 8 * su.shape[0] * su.shape[1] * su.shape[2] for su in setups)
+    e2e = {"value": world * cells * args.steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
+           "sequence": f"48 x mhd3d_upload (pinned) + mhd3d_ensemble_step({args.steps}) + mhd3d_ensemble_sync "
+                       f"+ 48 x mhd3d_download (pinned)", "ms": ms_e2e}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: members set up by the host mirror of STATIC/TUBE model 4/RAN2",
+                "config": {"workload": ENSEMBLE_NAME, "members": len(setups), "cells": cells,
+                           "tuned": tuned, "l2": "state 1.5 GB in HBM >> 126 MB L2, no flush needed",
+                           "parallelism": f"{world} independent ensemble replica(s), one per GPU, no collectives",
+                           "nit": [int(x) for x in res["nit"][:4]], "status_nonzero": int((res["status"] != 0).sum())},
+                "roofline": roof, "cpu_baseline": None, "e2e": e2e,
+                "gpu_launches": 4 * args.steps, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ens.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_closure(args, rank, world, local):
+    """The coarse side of the headline comparison: 128x128x64 FP32 with the
+    learned closure attached (evaluated every step: features, three tcgen05
+    convolutions, tendencies), same physics as the fine workload.  Also
+    reports the fine-equivalent rate 512^2*256 * (DT_coarse/DT_fine) /
+    wall, which assumes the closure holds the fine run's flux error."""
+    import torch
+    import mhd3d
+    import closure
+
+    w = dict(WORKLOAD)
+    cfg = mhd3d.convection_config(128, 128, 64, w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"], w["m"],
+                                  w["beta"], w["stretch"], w["ampt"], seed=62659 + rank)
+    setup = mhd3d.make_setup(cfg)
+    cells = 128 * 128 * 64
+    sim = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(setup.state)
+    net = closure.ClosureNet(seed=0)
+    net.attach(sim, trip=1e30)
+    sim.step(args.warmup)
+    clocks = ClockSampler(local) if rank == 0 else None
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    res = sim.sync()
+    clk = clocks.stop() if clocks else None
+    status = sim.closure_status()
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    # DT of the fine 512x512x256 run from the same initial physics (one CFL pass)
+    fcfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
+                                   w["m"], w["beta"], w["stretch"], w["ampt"], seed=62659 + rank)
+    fsetup = mhd3d.make_setup(fcfg)
+    fine = mhd3d.GpuSim(fsetup, mode=mhd3d.MODE_FAST)
+    fine.upload(fsetup.state)
+    dt_fine, _ = fine.cfl()
+    fine.close()
+    dt_coarse = res["dt"]
+    fine_cells = w["npx"] * w["npy"] * w["npz"]
+    fine_equiv = fine_cells * (dt_coarse / dt_fine) * args.steps / (ms / 1e3) / 1e6
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+                "data": "synthetic: rotating MHD polytrope from the host mirror of STATIC/TUBE model 4/RAN2; "
+                        "network weights seeded, not trained (throughput does not depend on them)",
+                "config": {"workload": "FP32+closure coarse run of the closure case: 128x128x64, same physics as "
+                                       "the 512x512x256 fine workload",
+                           "closure": {"evals": status["evals"], "trips": status["trips"], "err": status["err"]},
+                           "dt_coarse": dt_coarse, "dt_fine_first_step": dt_fine,
+                           "fine_equivalent_mcell_steps_per_s": fine_equiv,
+                           "fine_equivalent_note": "512^2*256 cells x (DT_coarse/DT_fine) per coarse step; assumes "
+                                                   "the closure holds the fine run's flux error (not demonstrated)",
+                           "parallelism": f"{world} independent replica(s), one per GPU, no collectives"},
+                "roofline": None, "cpu_baseline": None,
+                "e2e": None, "gpu_launches": 10 * args.steps, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -195,6 +391,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-npz", type=int, default=SAMPLE_NPZ)
+    ap.add_argument("--workload", choices=["fine", "ensemble", "closure"], default="fine",
+                    help="fine: the 512x512x256 step (default); ensemble: the batched FP32 ensemble "
+                         "of 48 uneven grids; closure: the FP32+closure coarse 128x128x64 run")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -214,6 +413,10 @@ def main():
     import mhd3d
 
     torch.cuda.set_device(local)
+    if args.workload == "ensemble":
+        return run_ensemble(args, rank, world, local)
+    if args.workload == "closure":
+        return run_closure(args, rank, world, local)
     dist = None
     if world > 1:
         import datetime
@@ -345,7 +548,7 @@ def main():
                 "data": "synthetic: rotating MHD polytrope from the host mirror of STATIC/TUBE model 4/RAN2",
                 "config": {"workload": WORKLOAD_NAME, "grid": [w["npx"], w["npy"], w["npz"]],
                            "mode": args.mode, "fields": nf,
-                           "l2": f"state {3 * nf * cells * 8 / 1e9:.1f} GB in HBM >> 126 MB L2, no flush needed",
+                           "l2": f"state {3 * nf * cells * word / 1e9:.1f} GB in HBM >> 126 MB L2, no flush needed",
                            "parallelism": f"{world} independent replica(s), one per GPU, no collectives",
                            "last_dt": res["dt"], "nit": res["nit"]},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,

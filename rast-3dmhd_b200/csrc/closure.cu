@@ -17,7 +17,10 @@
 //    weights stay in shared memory in the same canonical layout for all rows
 //    of the persistent CTA.  The accumulator is read back with tcgen05.ld;
 //    the epilogue adds the bias, applies ReLU or the ReLU mask of the layer
-//    below, and writes BF16 (and FP32) outputs.
+//    below, and writes BF16 (and FP32) outputs.  A CTA walks a contiguous run
+//    of rows along y and keeps a ring of four y rows (each with its z
+//    neighbours): a tile loads one new row, by cp.async, while the previous
+//    tile's MMAs run, and the taps address the ring's slots.
 //  - k_conv3d_wgrad: dW[n][tap*CIN+ci] = sum over voxels of dY[v][n] *
 //    X[v+tap][ci], an FP32 CUDA-core reduction (its M = COUT is below the
 //    64 rows of a tcgen05 instruction and its K runs over all voxels).
@@ -111,34 +114,68 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// load the input block of tile (x0, y, z): [chunk][voxel] 16-byte rows
-template <int CIN>
-__device__ __forceinline__ void load_block(unsigned char* sx, const __nv_bfloat16* __restrict__ x, int x0, int y,
-                                           int z, int nx, int ny, int nz)
+// Issue the asynchronous copies of the input block of tile (x0, y, z) into sx:
+// [chunk][voxel] 16-byte rows, periodic in x and y, zeros outside in z (a
+// zero-byte source fills zeros).  The caller commits and waits for the group.
+template <int CIN, int NTH>
+__device__ __forceinline__ void load_block_async(unsigned char* sx, const __nv_bfloat16* __restrict__ x, int x0,
+                                                 int y, int z, int nx, int ny, int nz)
 {
     constexpr int NC = CIN / 8;
-    for (int q = threadIdx.x; q < VB * NC; q += CT) {
+    const uint32_t sbase = smem_u32(sx);
+    for (int q = threadIdx.x; q < VB * NC; q += NTH) {
         const int c = q / VB, v = q % VB;
         const int xi = v % BX, yi = (v / BX) % 3, zi = v / (BX * 3);
         int gx = x0 - 1 + xi;
         gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
         int gy = y - 1 + yi;
         gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
-        const int gz = z - 1 + zi;
-        uint4 val = make_uint4(0u, 0u, 0u, 0u);
-        if (gz >= 0 && gz < nz)
-            val = *reinterpret_cast<const uint4*>(x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8);
-        *reinterpret_cast<uint4*>(sx + ((size_t)c * VB + v) * 16) = val;
+        int gz = z - 1 + zi;
+        const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
+        gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
+        const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sbase + (uint32_t)((c * VB + v) * 16)),
+                     "l"(src), "r"(nbytes)
+                     : "memory");
     }
 }
+// Ring of y rows for the convolution: [chunk][slot 0..3][z plane 0..2][BX voxels]
+// of 16-byte rows; row yr (unwrapped) lives in slot yr & 3.
+constexpr int RSEG = 4 * 3 * BX;   // voxel rows of one chunk of the ring
+template <int CIN, int NTH>
+__device__ __forceinline__ void load_row_async(unsigned char* ring, const __nv_bfloat16* __restrict__ x, int x0,
+                                               int yr, int z, int nx, int ny, int nz)
+{
+    constexpr int NC = CIN / 8;
+    const int slot = yr & 3;
+    int gy = yr % ny;
+    gy = gy < 0 ? gy + ny : gy;
+    const uint32_t sbase = smem_u32(ring);
+    for (int q = threadIdx.x; q < 3 * BX * NC; q += NTH) {
+        const int c = q / (3 * BX), r = q % (3 * BX);
+        const int zi = r / BX, xi = r % BX;
+        int gx = x0 - 1 + xi;
+        gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        int gz = z - 1 + zi;
+        const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
+        gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
+        const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8;
+        const uint32_t dst = sbase + (uint32_t)((c * RSEG + (slot * 3 + zi) * BX + xi) * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(nbytes) : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <int CIN, int COUT>
 struct ConvLay {
     static constexpr int K = 27 * CIN;
     static constexpr size_t W_B = (size_t)COUT * K * 2;
     static constexpr size_t X_OFF = (W_B + 127) / 128 * 128;
-    static constexpr size_t X_B = (size_t)CIN * VB * 2;
-    static constexpr size_t BAR_OFF = (X_OFF + X_B + 127) / 128 * 128;
+    static constexpr size_t X_B = ((size_t)CIN * RSEG * 2 + 127) / 128 * 128;  // ring of four y rows
+    static constexpr size_t BAR_OFF = X_OFF + X_B;
     static constexpr size_t BYTES = BAR_OFF + 16 + 128;
 };
 
@@ -182,25 +219,43 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
+    // tiles in (segment, z, y) order with y fastest; each CTA takes one
+    // contiguous run, so consecutive tiles share two of their three y rows
     const int nseg = nx / MT;
     const int ntile = nseg * ny * nz;
     constexpr uint32_t IDESC = idesc_bf16(MT, COUT);
-    const uint32_t sx_a = smem_u32(sx), sw_a = smem_u32(sw);
+    const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
+    const int t_begin = (int)(((long)ntile * blockIdx.x) / gridDim.x);
+    const int t_end = (int)(((long)ntile * (blockIdx.x + 1)) / gridDim.x);
+    auto tile_of = [&](int t, int& x0, int& yy, int& zz) {
+        yy = t % ny;
+        zz = (t / ny) % nz;
+        x0 = (t / (ny * nz)) * MT;
+    };
     unsigned phase = 0;
     bool failed = false;
-    for (int t = blockIdx.x; t < ntile && !failed; t += gridDim.x) {
-        const int seg = t % nseg, yy = (t / nseg) % ny, zz = t / (nseg * ny);
-        const int x0 = seg * MT;
-        load_block<CIN>(sx, x, x0, yy, zz, nx, ny, nz);
-        fence_proxy_async();     // generic-proxy stores -> visible to the tensor core
+    for (int t = t_begin; t < t_end && !failed; ++t) {
+        int x0, yy, zz;
+        tile_of(t, x0, yy, zz);
+        const bool fresh = t == t_begin || yy == 0;   // a new (segment, z) run: rows y-1, y, y+1
+        if (fresh) {
+            for (int d = -1; d <= 1; ++d) load_row_async<CIN, CT>(sx, x, x0, yy + d, zz, nx, ny, nz);
+            cp_async_commit();
+        }
+        // the next tile's new row streams in while this tile is multiplied
+        if (t + 1 < t_end && yy + 1 < ny) load_row_async<CIN, CT>(sx, x, x0, yy + 2, zz, nx, ny, nz);
+        cp_async_commit();
+        cp_async_wait<1>();
+        fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
             for (int tap = 0; tap < 27; ++tap) {
-                const int v0 = (tap % 3) + BX * ((tap / 3) % 3) + BX * 3 * (tap / 9);
+                const int dxi = tap % 3, dyi = (tap / 3) % 3, dzi = tap / 9;
+                const int row = ((((yy + dyi - 1) & 3) * 3 + dzi) * BX + dxi);
 #pragma unroll
                 for (int kk = 0; kk < CIN / 16; ++kk) {
-                    const uint64_t da = smem_desc(sx_a + (uint32_t)((2 * kk) * VB + v0) * 16u, VB * 16, 128);
+                    const uint64_t da = smem_desc(sx_a + (uint32_t)((2 * kk) * RSEG + row) * 16u, RSEG * 16, 128);
                     const uint64_t db = smem_desc(sw_a + (uint32_t)((tap * CIN + kk * 16) >> 3) * 128u, 128,
                                                   (K / 8) * 128);
                     umma_bf16(tmem, da, db, IDESC, (tap | kk) != 0 ? 1u : 0u);
@@ -245,6 +300,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
         tc_fence_before();
         __syncthreads();
     }
+    cp_async_wait<0>();
     tc_fence_after();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
 }
@@ -273,21 +329,11 @@ __global__ void __launch_bounds__(COUT * CIN / 4) k_conv3d_wgrad(const __nv_bflo
         const int seg = t % nseg, yy = (t / nseg) % ny, zz = t / (nseg * ny);
         const int x0 = seg * MT;
         __syncthreads();
-        for (int q = threadIdx.x; q < VB * (CIN / 8); q += NTH) {
-            const int c = q / VB, v = q % VB;
-            const int xi = v % BX, yi = (v / BX) % 3, zi = v / (BX * 3);
-            int gx = x0 - 1 + xi;
-            gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
-            int gy = yy - 1 + yi;
-            gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
-            const int gz = zz - 1 + zi;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            if (gz >= 0 && gz < nz)
-                val = *reinterpret_cast<const uint4*>(x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8);
-            *reinterpret_cast<uint4*>(sx + ((size_t)c * VB + v) * 16) = val;
-        }
+        load_block_async<CIN, NTH>(sx, x, x0, yy, zz, nx, ny, nz);
+        cp_async_commit();
         const size_t row = ((size_t)zz * ny + yy) * nx + x0;
         for (int q = threadIdx.x; q < MT * COUT; q += NTH) sdy[q] = __bfloat162float(dy[row * COUT + q]);
+        cp_async_wait<0>();
         __syncthreads();
         // channels 4*c4..4*c4+3 live in chunk c4/2, halves (c4%2)
         const unsigned char* xb = sx + (size_t)(c4 >> 1) * VB * 16 + (c4 & 1) * 8;
