@@ -112,6 +112,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(ms: float, dist) -> float:
+    """The slowest rank's time (every rank takes the same collective)."""
+    if dist is None:
+        return ms
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(cells_per_rank: int, steps: int, ms: float, world: int) -> float:
+    """Whole-job Mcell-RK3-steps/s: all ranks' cells x steps over the slowest rank's time."""
+    return world * cells_per_rank * steps / (ms / 1e3) / 1e6
+
+
 def pow2_floor(n):
     p = 1
     while p * 2 <= n:
@@ -246,10 +262,7 @@ def run_ensemble(args, rank, world, local):
     res = ens.sync()
     barrier()
     clk = clocks.stop() if clocks else None
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     value = world * cells * args.steps / (ms / 1e3) / 1e6
     peaks, peak_src = measured_peaks()
     achieved = cells * 320.0 * args.steps / (ms / 1e3) / 1e9
@@ -467,11 +480,8 @@ def main():
     clk = clocks.stop() if clocks else None
     stage_ms, stage_n = sim.profile_read()
     sim.profile(False)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, dist)
+    value = aggregate_rate(cells, args.steps, ms, world)
 
     # roofline of the fused stage kernel
     peaks, peak_src = measured_peaks()
@@ -521,10 +531,7 @@ def main():
     f1.synchronize()
     wall_e2e = time.perf_counter() - wt0
     ms_e2e = max(f0.elapsed_time(f1), wall_e2e * 1e3)
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dist)
     state_bytes = nf * nfort * 8
     e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / e2e_steps,
