@@ -282,7 +282,7 @@ int mhd3d_ensemble_set_stream(void* ens, void* stream);
  * arrays are device pointers; activations are channels-last BF16
  * [nz][ny][nx][C] (periodic in x and y, zero outside in z), weights BF16
  * [cout][27*cin] with k = tap*cin + ci, tap = (dx+1) + 3*(dy+1) + 9*(dz+1).
- * nx must be a multiple of 128.  Supported (cin, cout): (16,32), (32,32),
+ * nx must be a multiple of 128 or divide 128.  Supported (cin, cout): (16,32), (32,32),
  * (32,16).  Work is enqueued on stream; err (device int) is set non-zero if
  * a bounded wait of the tensor-core pipeline gave up.
  *
@@ -301,7 +301,7 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
                        int32_t ny, int32_t nz, void* stream);
 
 /*
- * Learned closure on an FP32 handle whose NPX is a multiple of 128.
+ * Learned closure on an FP32 handle whose NPX is a multiple of 128 or divides 128.
  * mhd3d_closure_set attaches a trained network (weights BF16 [cout][27*cin]:
  * w1 32x432, w2 32x864, w3 16x864; biases FP32 32, 32, 16; in_scale[8] the
  * feature scales; out_scale[12] the target scales; host or device pointers,

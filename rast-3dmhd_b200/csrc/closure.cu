@@ -127,7 +127,8 @@ __device__ __forceinline__ void load_block_async(unsigned char* sx, const __nv_b
         const int c = q / VB, v = q % VB;
         const int xi = v % BX, yi = (v / BX) % 3, zi = v / (BX * 3);
         int gx = x0 - 1 + xi;
-        gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        if (nx >= MT) gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        else gx = (gx + nx) % nx;   // a 128-point tile spans 128/nx periods
         int gy = y - 1 + yi;
         gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
         int gz = z - 1 + zi;
@@ -155,7 +156,8 @@ __device__ __forceinline__ void load_row_async(unsigned char* ring, const __nv_b
         const int c = q / (3 * BX), r = q % (3 * BX);
         const int zi = r / BX, xi = r % BX;
         int gx = x0 - 1 + xi;
-        gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        if (nx >= MT) gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        else gx = (gx + nx) % nx;   // a 128-point tile spans 128/nx periods
         int gz = z - 1 + zi;
         const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
         gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
 
     // tiles in (segment, z, y) order with y fastest; each CTA takes one
     // contiguous run, so consecutive tiles share two of their three y rows
-    const int nseg = nx / MT;
+    const int nseg = (nx + MT - 1) / MT;
     const int ntile = nseg * ny * nz;
     constexpr uint32_t IDESC = idesc_bf16(MT, COUT);
     const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
@@ -273,7 +275,8 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
             float acc[COUT];
             tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), acc);
             const int m = warp * 32 + lane;
-            const size_t vox = ((size_t)zz * ny + yy) * nx + x0 + m;
+            const bool own = x0 + m < nx;   // for nx < 128 the tile repeats the row's period
+            const size_t vox = ((size_t)zz * ny + yy) * nx + (own ? x0 + m : 0);
 #pragma unroll
             for (int n = 0; n < COUT; ++n) {
                 float o = acc[n] + (bias ? bias[n] : 0.f);
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
                 if (mask && !(__bfloat162float(mask[vox * COUT + n]) > 0.f)) o = 0.f;
                 acc[n] = o;
             }
-            if (y) {
+            if (y && own) {
 #pragma unroll
                 for (int n = 0; n < COUT; n += 8) {
                     __align__(16) __nv_bfloat16 h[8];
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
                     *reinterpret_cast<uint4*>(y + vox * COUT + n) = *reinterpret_cast<const uint4*>(h);
                 }
             }
-            if (yf) {
+            if (yf && own) {
 #pragma unroll
                 for (int n = 0; n < COUT; n += 4)
                     *reinterpret_cast<float4*>(yf + vox * COUT + n) =
@@ -323,7 +326,7 @@ __global__ void __launch_bounds__(COUT * CIN / 4) k_conv3d_wgrad(const __nv_bflo
 #pragma unroll
     for (int t = 0; t < 27; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
     float bacc = 0.f;
-    const int nseg = nx / MT;
+    const int nseg = (nx + MT - 1) / MT;
     const int ntile = nseg * ny * nz;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
         const int seg = t % nseg, yy = (t / nseg) % ny, zz = t / (nseg * ny);
@@ -332,12 +335,13 @@ __global__ void __launch_bounds__(COUT * CIN / 4) k_conv3d_wgrad(const __nv_bflo
         load_block_async<CIN, NTH>(sx, x, x0, yy, zz, nx, ny, nz);
         cp_async_commit();
         const size_t row = ((size_t)zz * ny + yy) * nx + x0;
-        for (int q = threadIdx.x; q < MT * COUT; q += NTH) sdy[q] = __bfloat162float(dy[row * COUT + q]);
+        const int mlim = nx - x0 < MT ? nx - x0 : MT;   // voxels of this tile that are the row's own
+        for (int q = threadIdx.x; q < mlim * COUT; q += NTH) sdy[q] = __bfloat162float(dy[row * COUT + q]);
         cp_async_wait<0>();
         __syncthreads();
         // channels 4*c4..4*c4+3 live in chunk c4/2, halves (c4%2)
         const unsigned char* xb = sx + (size_t)(c4 >> 1) * VB * 16 + (c4 & 1) * 8;
-        for (int m = 0; m < MT; ++m) {
+        for (int m = 0; m < mlim; ++m) {
             const float g = sdy[m * COUT + n];
             bacc += g;
 #pragma unroll
@@ -387,7 +391,7 @@ cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ntile = (nx / MT) * ny * nz;
+    const int ntile = ((nx + MT - 1) / MT) * ny * nz;
     const int grid = ntile < sms ? ntile : sms;
     k_conv3d<CIN, COUT><<<grid, CT, L::BYTES, st>>>(
         static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
@@ -409,7 +413,7 @@ cudaError_t launch_wgrad_t(const void* x, const void* dy, float* dw, float* db, 
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ntile = (nx / MT) * ny * nz;
+    const int ntile = ((nx + MT - 1) / MT) * ny * nz;
     const int grid = ntile < 2 * sms ? ntile : 2 * sms;
     k_conv3d_wgrad<CIN, COUT><<<grid, COUT * CIN / 4, smem, st>>>(
         static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, db, nx, ny, nz);
@@ -426,7 +430,8 @@ extern "C" {
 int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const float* bias, const void* mask,
                  int32_t relu, void* y, float* yf, int32_t nx, int32_t ny, int32_t nz, int32_t* err, void* stream)
 {
-    if (!x || !w || !err || nx <= 0 || nx % MT || ny <= 0 || nz <= 0 || (!y && !yf)) return MHD3D_ERR_ARG;
+    if (!x || !w || !err || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0 || (!y && !yf))
+        return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (cin == 16 && cout == 32) e = launch_conv_t<16, 32>(x, w, bias, mask, relu, y, yf, nx, ny, nz, err, st);
@@ -439,7 +444,7 @@ int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const 
 int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, float* db, int32_t nx,
                        int32_t ny, int32_t nz, void* stream)
 {
-    if (!x || !dy || !dw || nx <= 0 || nx % MT || ny <= 0 || nz <= 0) return MHD3D_ERR_ARG;
+    if (!x || !dy || !dw || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (cin == 16 && cout == 32) e = launch_wgrad_t<16, 32>(x, dy, dw, db, nx, ny, nz, st);

@@ -27,7 +27,9 @@ def _p(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
-SHAPES = [((5, 6, 128), 16, 32), ((4, 3, 256), 32, 32), ((3, 5, 128), 32, 16)]
+# x periods of 128 and 256, and 64 and 32: a 128-point tile then spans several periods
+SHAPES = [((5, 6, 128), 16, 32), ((4, 3, 256), 32, 32), ((3, 5, 128), 32, 16),
+          ((4, 6, 64), 16, 32), ((3, 4, 32), 32, 32), ((5, 3, 64), 32, 16)]
 
 
 @pytest.mark.parametrize("shape,cin,cout", SHAPES)
