@@ -174,7 +174,7 @@ class PairCollector:
         """The last snapshot's coarse state as Fortran arrays (host)."""
         sh = (self.shape[2] + 2, self.shape[1] + 2, self.shape[0] + 2)
         a = self.cstate.cpu().numpy()
-        out = {f: a[i * self.NC:(i + 1) * self.NC].reshape(sh, order="F").copy() for i, f in
+        out = {f: a[i * self.NC:(i + 1) * self.NC].reshape(sh, order="F").copy(order="F") for i, f in
                enumerate(mhd3d.FIELDS[:self.nf])}
         for f in mhd3d.FIELDS[self.nf:]:
             out[f] = None

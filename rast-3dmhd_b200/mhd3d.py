@@ -147,6 +147,18 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def field_array(a, shape):
+    """A field as the C-ABI reads it: float64, Fortran order, shape (NX,NY,NZ).
+    Arrays in another memory order are copied (index order is kept), so a
+    C-ordered array is never read transposed."""
+    if a is None:
+        return None
+    a = np.asarray(a)
+    if a.shape != tuple(shape):
+        raise ValueError(f"field shape {a.shape} != {tuple(shape)}")
+    return np.asfortranarray(a, dtype=np.float64)
+
+
 GRID_NAMES = ("exx", "dxxdx", "d2xxdx2", "ddx", "wyy", "dyydy", "d2yydy2", "ddy",
               "zee", "dzzdz", "d2zzdz2", "ddz", "rkapa", "dkapa")
 
@@ -249,7 +261,8 @@ class GpuSim:
             pass
 
     def upload(self, state: dict):
-        st = self.lib.mhd3d_upload(self.h, *[_ptr(state.get(f)) for f in FIELDS])
+        arrs = [field_array(state.get(f), self.setup.shape) for f in FIELDS]
+        st = self.lib.mhd3d_upload(self.h, *[_ptr(a) for a in arrs])
         if st:
             raise Mhd3dError(st, "mhd3d_upload")
 

@@ -103,3 +103,18 @@ def test_dimensionless_mapping(mhd3d):
     rho_mid = 5.5
     assert abs(cfg.ry - cfg.re * rho_mid / 100.0) < 1e-12 * cfg.ry
     assert abs(cfg.rm - 4.0 * cfg.re * rho_mid) < 1e-12 * cfg.rm
+
+
+def test_field_array_keeps_index_order(mhd3d):
+    """A C-ordered field is copied to Fortran order, never read transposed."""
+    import numpy as np
+    a = np.arange(4 * 3 * 2, dtype=np.float32).reshape(4, 3, 2)   # C order
+    f = mhd3d.field_array(a, (4, 3, 2))
+    assert f.flags.f_contiguous and f.dtype == np.float64
+    assert np.array_equal(f, a)
+    g = np.asfortranarray(a, dtype=np.float64)
+    assert mhd3d.field_array(g, (4, 3, 2)) is g or np.shares_memory(mhd3d.field_array(g, (4, 3, 2)), g)
+    assert mhd3d.field_array(None, (4, 3, 2)) is None
+    import pytest
+    with pytest.raises(ValueError):
+        mhd3d.field_array(a, (2, 3, 4))
