@@ -336,6 +336,22 @@ int mhd3d_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr
 int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_scale, float* out, int32_t* flag,
                            float trip, void* stream);
 
+/*
+ * Training the closure on tendencies (no counterpart in the reference): a
+ * target given as the 7 tendencies a coarse run misses (for instance the
+ * filtered fine run's rate of change minus the coarse scheme's right-hand
+ * sides) is fitted through the same stress, heat-flux and EMF outputs.
+ * mhd3d_closure_tendency_loss: loss += sum_f weight[f] * sum (tend -
+ * target)^2 / (7 nvox) over arrays [7][nvox] (device), and g = d loss /
+ * d tend.  mhd3d_closure_tendency_adjoint: the transpose of
+ * mhd3d_closure_tendency's map for the handle's state, g [7][nvox] ->
+ * dpred [nvox][16] BF16 (channels 12..15 zero), the gradient to feed the
+ * network's last layer.
+ */
+int mhd3d_closure_tendency_loss(const float* tend, const float* target, const float* weight, int64_t nvox, float* g,
+                                double* loss, void* stream);
+int mhd3d_closure_tendency_adjoint(void* handle, const float* g, const float* out_scale, void* dpred, void* stream);
+
 const char* mhd3d_version(void);
 
 #ifdef __cplusplus

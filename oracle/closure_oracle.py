@@ -58,3 +58,80 @@ def conv3d_dw(x, dy):
     for tap, dx, ddy, dz in _taps():
         dw[:, tap * cin:(tap + 1) * cin] = g.T @ _shift(x, dx, ddy, dz).reshape(-1, cin)
     return dw, g.sum(axis=0)
+
+
+# -- closure tendencies -------------------------------------------------------
+# The tendencies the coarse run adds to its right-hand sides from the
+# network's 12 outputs P (stress tau_xx, tau_yy, tau_zz, tau_xy, tau_xz,
+# tau_yz; heat flux q_x, q_y, q_z; EMF eps_x, eps_y, eps_z, each times its
+# scale): centred differences with the grid's metric factors, periodic in x
+# and y, zero on the first and last z plane.  Output fields RU, RV, RW, TT,
+# BX, BY, BZ.  (field, direction, sign) of every output channel; TT's terms
+# are also divided by the cell's density.
+TEND_TERMS = {
+    0: [(0, 0, -1.0)], 1: [(1, 1, -1.0)], 2: [(2, 2, -1.0)],
+    3: [(0, 1, -1.0), (1, 0, -1.0)], 4: [(0, 2, -1.0), (2, 0, -1.0)], 5: [(1, 2, -1.0), (2, 1, -1.0)],
+    6: [(3, 0, -1.0)], 7: [(3, 1, -1.0)], 8: [(3, 2, -1.0)],
+    9: [(5, 2, 1.0), (6, 1, -1.0)], 10: [(6, 0, 1.0), (4, 2, -1.0)], 11: [(4, 1, 1.0), (5, 0, -1.0)],
+}
+
+
+def _metric(ax, ay, az, d, shape):
+    nz, ny, nx = shape
+    if d == 0:
+        return np.broadcast_to(np.asarray(ax)[None, None, :], shape)
+    if d == 1:
+        return np.broadcast_to(np.asarray(ay)[None, :, None], shape)
+    return np.broadcast_to(np.asarray(az)[:, None, None], shape)
+
+
+def _cdiff(a, d):
+    """a[n+1] - a[n-1] along axis d of [z][y][x] (2 - d); periodic in x, y."""
+    axis = 2 - d
+    if d < 2:
+        return np.roll(a, -1, axis=axis) - np.roll(a, 1, axis=axis)
+    out = np.zeros_like(a)
+    out[1:-1] = a[2:] - a[:-2]
+    return out
+
+
+def tendency_fwd(pred, osc, ax, ay, az, ro):
+    """pred [z][y][x][>=12] (normalised outputs), osc[12] scales, ax[nx],
+    ay[ny], az[nz] metric factors of the cells, ro [z][y][x] density.
+    Returns [7][z][y][x]."""
+    shape = pred.shape[:3]
+    out = np.zeros((7,) + shape)
+    for c, terms in TEND_TERMS.items():
+        p = np.asarray(pred[..., c], dtype=np.float64) * float(osc[c])
+        for f, d, s in terms:
+            t = s * _cdiff(p, d) * _metric(ax, ay, az, d, shape)
+            out[f] += t / ro if f == 3 else t
+    out[:, 0] = 0.0
+    out[:, -1] = 0.0
+    return out
+
+
+def tendency_adj(g, osc, ax, ay, az, ro):
+    """Adjoint of tendency_fwd: g [7][z][y][x] -> dpred [z][y][x][16]."""
+    shape = g.shape[1:]
+    gi = np.array(g, dtype=np.float64)
+    gi[:, 0] = 0.0
+    gi[:, -1] = 0.0
+    out = np.zeros(shape + (16,))
+    for c, terms in TEND_TERMS.items():
+        acc = np.zeros(shape)
+        for f, d, s in terms:
+            h = gi[f] * _metric(ax, ay, az, d, shape)
+            if f == 3:
+                h = h / ro
+            # adjoint of a[n+1] - a[n-1]: h[m-1] - h[m+1]
+            axis = 2 - d
+            if d < 2:
+                acc += s * (np.roll(h, 1, axis=axis) - np.roll(h, -1, axis=axis))
+            else:
+                t = np.zeros(shape)
+                t[1:] += h[:-1]
+                t[:-1] -= h[1:]
+                acc += s * t
+        out[..., c] = acc * float(osc[c])
+    return out

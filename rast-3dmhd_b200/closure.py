@@ -11,8 +11,9 @@ Every arithmetic step runs in the library (libmhd3d_gpu.so): coarsening and
 targets (mhd3d_coarsen), features, the tcgen05 convolutions and their input
 gradients (mhd3d_conv3d, mhd3d_conv3d_wtranspose), FP32 weight gradients
 (mhd3d_conv3d_wgrad), the loss and its gradient (mhd3d_closure_loss), Adam
-(mhd3d_adam) and the closure tendencies (mhd3d_closure_tendency).  torch
-provides device memory and streams only.
+(mhd3d_adam), the closure tendencies (mhd3d_closure_tendency) and, for
+training on tendencies, their loss and adjoint (mhd3d_closure_tendency_loss,
+mhd3d_closure_tendency_adjoint).  torch provides device memory and streams.
 """
 from __future__ import annotations
 
@@ -107,6 +108,13 @@ class ClosureNet:
                                          _p(self.err), C.c_void_p(stream)), "mhd3d_conv3d (input gradient)")
             dy = dx
 
+    def reset_optimizer(self):
+        """Zero Adam's moments and step count (before training on a new loss)."""
+        for mv in self.m + self.v:
+            for t in mv:
+                t.zero_()
+        self.t = 0
+
     def zero_grad(self):
         for g in self.dw + self.db:
             g.zero_()
@@ -128,6 +136,26 @@ class ClosureNet:
         dy = torch.empty(pred.shape[:3] + (16,), dtype=torch.bfloat16, device="cuda")
         _check(self.lib.mhd3d_closure_loss(_p(pred), _p(target), nvox, _p(dy), _p(loss), C.c_void_p(stream)),
                "mhd3d_closure_loss")
+        return loss, dy
+
+    def tendency_loss_and_grad(self, sim, pred, target, weight, stream):
+        """Loss of the closure tendencies of pred (for sim's current state)
+        against target [7, nz, ny, nx] with per-field weights [7], and its
+        gradient with respect to pred as the last layer's dy (BF16)."""
+        torch = _torch()
+        nz, ny, nx = pred.shape[:3]
+        nvox = nz * ny * nx
+        tend = torch.empty((7, nz, ny, nx), dtype=torch.float32, device="cuda")
+        flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _check(self.lib.mhd3d_closure_tendency(sim.h, _p(pred), _p(self.out_scale), _p(tend), _p(flag),
+                                               C.c_float(1e30), C.c_void_p(stream)), "mhd3d_closure_tendency")
+        g = torch.empty_like(tend)
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        _check(self.lib.mhd3d_closure_tendency_loss(_p(tend), _p(target), _p(weight), nvox, _p(g), _p(loss),
+                                                    C.c_void_p(stream)), "mhd3d_closure_tendency_loss")
+        dy = torch.empty((nz, ny, nx, 16), dtype=torch.bfloat16, device="cuda")
+        _check(self.lib.mhd3d_closure_tendency_adjoint(sim.h, _p(g), _p(self.out_scale), _p(dy), C.c_void_p(stream)),
+               "mhd3d_closure_tendency_adjoint")
         return loss, dy
 
     def attach(self, sim: mhd3d.GpuSim, trip: float = 1.0):
@@ -161,14 +189,18 @@ class PairCollector:
         _check(self.lib.mhd3d_coarsen(fine.h, self.fac, _p(self.cstate), _p(tg), C.c_void_p(self.stream)),
                "mhd3d_coarsen")
         torch.cuda.synchronize()
-        ptrs = [C.c_void_p(self.cstate.data_ptr() + 8 * self.NC * i) for i in range(self.nf)]
-        ptrs += [None] * (8 - self.nf)
-        _check(self.lib.mhd3d_upload(self.coarse.h, *ptrs), "mhd3d_upload")
+        self.load(self.cstate)
         feat = torch.empty((nz, ny, nx, 16), dtype=torch.bfloat16, device="cuda")
         _check(self.lib.mhd3d_closure_features(self.coarse.h, _p(in_scale), _p(feat), _p(self.means),
                                                C.c_void_p(self.stream)), "mhd3d_closure_features")
         torch.cuda.synchronize()
         return feat, tg
+
+    def load(self, cstate):
+        """Upload a filtered state (device, as mhd3d_coarsen writes it) into the coarse handle."""
+        ptrs = [C.c_void_p(cstate.data_ptr() + 8 * self.NC * i) for i in range(self.nf)]
+        ptrs += [None] * (8 - self.nf)
+        _check(self.lib.mhd3d_upload(self.coarse.h, *ptrs), "mhd3d_upload")
 
     def coarse_state(self):
         """The last snapshot's coarse state as Fortran arrays (host)."""

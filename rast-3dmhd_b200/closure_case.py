@@ -19,6 +19,13 @@ Pipeline (every arithmetic step in libmhd3d_gpu.so; torch holds device memory):
    sampling excluded) gives the wall-time ratio of the fine run to the coarse
    run with the closure.
 
+With ``--resid-steps N`` the network trained on the filter commutator is
+then fine-tuned on the coarse scheme's residual: at each sample the fine run
+is advanced N more steps, and R = (B - A)/(tB - tA) - (F(A) + F(B))/2 of the
+filtered states A, B and the coarse FP32 right-hand side F is what the
+closure tendencies are fitted to (what the coarse method misses in total,
+truncation error included, not only the subgrid terms).
+
 Prints one JSON object: per-profile relative L2 errors of the time-averaged
 profiles (plain coarse and closure coarse against filtered fine), the closure's
 trip count, the a-priori tendency error on the judge run's last pair, step
@@ -75,6 +82,46 @@ def advance_to(sim, t_target, chunk, log=None, tag="", last=None):
             return steps, wall, r
 
 
+TEND_FIELDS = ((0, "fu"), (1, "fv"), (2, "fw"), (3, "ft"), (5, "ww1"), (6, "ww2"), (7, "ww3"))
+
+
+def residual_target(pc, fine, nsteps):
+    """The coarse scheme's residual at the collector's current filtered
+    state A: advance the fine run nsteps to B, and return
+    R = (B - A) / (tB - tA) - (F(A) + F(B)) / 2 for RU, RV, RW, TT, BX, BY, BZ
+    as [7, nz, ny, nx] FP32 on the device, where F is the coarse FP32
+    scheme's right-hand side (trapezoidal, so R is second order in tB - tA),
+    together with the filtered state A itself (device, as mhd3d_coarsen
+    writes it) and the fine run's step record at B."""
+    torch = _torch()
+    nz, ny, nx = pc.shape
+    sh = (nx + 2, ny + 2, nz + 2)
+    ta = pc.t_last
+    ca = pc.cstate.clone()
+    fa = pc.coarse.fluxes()
+    t0 = time.perf_counter()
+    r = fine.step(nsteps, check=False)
+    r["wall"] = time.perf_counter() - t0
+    if r["status"]:
+        raise mhd3d.Mhd3dError(r["status"], "fine residual steps")
+    pc.snapshot(fine, torch.ones(8, dtype=torch.float32, device="cuda"))
+    pc.t_last = r["timt"]
+    fb = pc.coarse.fluxes()
+    a, b = ca.cpu().numpy(), pc.cstate.cpu().numpy()
+    dt = r["timt"] - ta
+    out = np.zeros((7, nz, ny, nx))
+    for o, (fi, fn) in enumerate(TEND_FIELDS):
+        if fi >= pc.nf:
+            continue
+        A = a[fi * pc.NC:(fi + 1) * pc.NC].reshape(sh, order="F")[1:-1, 1:-1, 1:-1]
+        B = b[fi * pc.NC:(fi + 1) * pc.NC].reshape(sh, order="F")[1:-1, 1:-1, 1:-1]
+        rr = (B - A) / dt - 0.5 * (fa[fn] + fb[fn])[1:-1, 1:-1, 1:-1]
+        out[o] = np.transpose(rr, (2, 1, 0))
+    out[:, 0] = 0.0
+    out[:, -1] = 0.0
+    return torch.tensor(out, dtype=torch.float32, device="cuda"), ca, r
+
+
 def fine_phase(args, seed, collect, log):
     """Spin up a fine run, then sample the window.  Returns the filtered
     coarse state at the window start, the sampled pairs (all of them if
@@ -93,13 +140,19 @@ def fine_phase(args, seed, collect, log):
     if r["status"]:
         raise mhd3d.Mhd3dError(r["status"], "fine spin-up")
     t0 = r["timt"]
-    pairs, profs = [], []
+    pairs, profs, resid = [], [], []
     pair = pc.snapshot(fine, ones)
+    pc.t_last = r["timt"]
     start = pc.coarse_state()
     profs.append(pc.coarse.profiles())
     if collect:
         pairs.append(pair)
-    wsteps, wwall, dts, machs = 0, 0.0, [], []
+    wsteps, wwall = 0, 0.0
+    if args.resid_steps and collect:
+        R, ca, r = residual_target(pc, fine, args.resid_steps)
+        resid.append((R, ca))
+        wsteps, wwall = args.resid_steps, r["wall"]
+    dts, machs = [], []
     for s in range(1, args.samples + 1):
         n, w, r = advance_to(fine, t0 + args.window * s / args.samples, args.chunk, last=r)
         if r["status"]:
@@ -109,14 +162,22 @@ def fine_phase(args, seed, collect, log):
         dts.append(r["dt"])
         machs.append(r["umach"])
         pair = pc.snapshot(fine, ones)
+        pc.t_last = t_sample = r["timt"]
         profs.append(pc.coarse.profiles())
         if collect:
             pairs.append(pair)
+        if args.resid_steps and (collect or s == args.samples):
+            R, ca, r = residual_target(pc, fine, args.resid_steps)
+            resid.append((R, ca))
+            if collect:   # the judge's last target lies past its window
+                wsteps += args.resid_steps
+                wwall += r["wall"]
         log(f"fine{seed} sample {s} t={r['timt']:.4f} dt={r['dt']:.3e} umach={r['umach']:.3e}")
     if not collect:
         pairs = [pair]   # the last pair: its filtered state is resident in the collector
     fine.close()
-    return {"start": start, "pairs": pairs, "profiles": np.mean(profs, axis=0), "t0": t0, "t1": r["timt"],
+    return {"start": start, "pairs": pairs, "resid": resid, "profiles": np.mean(profs, axis=0), "t0": t0,
+            "t1": t_sample,
             "steps": wsteps, "wall": wwall, "spin_steps": steps, "dt_mean": float(np.mean(dts)),
             "umach_max": float(np.max(machs)), "pc": pc, "coarse_setup": cs}
 
@@ -148,7 +209,40 @@ def train(pairs, args, log):
             log(f"train it={it} loss={lv:.4e} lr={lr:.2e}")
     torch.cuda.synchronize()
     return net, {"iters": args.iters, "pairs": len(pairs), "loss_first": first, "loss_last": loss.item(),
-                 "seconds": time.perf_counter() - t0}
+                 "seconds": time.perf_counter() - t0}, data
+
+
+def train_residual(net, data, resid, pc, args, log):
+    """Fine-tune on the coarse scheme's residual: the closure tendencies of
+    the network's outputs are fitted to R by the tendency loss (fields
+    weighted by 1 / mean R_f^2) and its adjoint."""
+    torch = _torch()
+    msq = torch.stack([(R.double() ** 2).mean(dim=(1, 2, 3)) for R, _ in resid]).mean(dim=0)
+    w = (1.0 / msq.clamp_min(1e-300)).float()
+    w = (w * 7.0 / w.sum()).contiguous()
+    s = torch.cuda.current_stream().cuda_stream
+    shape = pc.shape
+    net.reset_optimizer()
+    t0 = time.perf_counter()
+    first = None
+    n = min(len(data), len(resid))
+    for it in range(args.resid_iters):
+        i = it % n
+        (f, _), (R, ca) = data[i], resid[i]
+        pc.load(ca)
+        net.zero_grad()
+        acts, p = net.forward(f, shape, s)
+        loss, dy = net.tendency_loss_and_grad(pc.coarse, p, R, w, s)
+        net.backward(acts, dy, shape, s)
+        lr = args.resid_lr * 0.5 * (1.0 + np.cos(np.pi * it / args.resid_iters))
+        net.adam_step(lr, s)
+        if it % 500 == 0 or it == args.resid_iters - 1:
+            lv = loss.item()
+            first = lv if first is None else first
+            log(f"residual it={it} loss={lv:.4e} lr={lr:.2e}")
+    torch.cuda.synchronize()
+    return {"iters": args.resid_iters, "pairs": n, "loss_first": first, "loss_last": loss.item(),
+            "seconds": time.perf_counter() - t0, "weights": w.cpu().tolist()}, w
 
 
 def a_priori(net, judge, log):
@@ -161,12 +255,29 @@ def a_priori(net, judge, log):
     pad = torch.cat([net.in_scale, torch.ones(8, device="cuda")])
     ones12 = torch.ones(12, device="cuda")
     f, t = judge["pairs"][-1]
+    if judge["resid"]:
+        pc.load(judge["resid"][-1][1])   # the pair's own filtered state
     _, p = net.forward((f.float()[..., :16] * pad).to(torch.bfloat16), pc.shape, s)
     true_t, _ = closure.tendencies(pc.coarse, closure.pad_targets(t, ones12), ones12)
     pred_t, _ = closure.tendencies(pc.coarse, p, net.out_scale)
     ratio = ((pred_t - true_t) ** 2).sum().item() / (true_t ** 2).sum().item()
     log(f"a priori tendency error ratio {ratio:.4f}")
-    return ratio
+    out = {"commutator_error_ratio": ratio}
+    if judge["resid"]:
+        # against the coarse scheme's residual at the same state (weighted as in training)
+        R, ca = judge["resid"][-1]
+        pc.load(ca)
+        _, p = net.forward((f.float()[..., :16] * pad).to(torch.bfloat16), pc.shape, s)
+        pred_t, _ = closure.tendencies(pc.coarse, p, net.out_scale)
+        true_t, _ = closure.tendencies(pc.coarse, closure.pad_targets(t, ones12), ones12)
+        w = judge.get("resid_w")
+        wv = (w if w is not None else torch.ones(7, device="cuda")).view(7, 1, 1, 1)
+        den = (wv * R ** 2).sum().item()
+        out["residual_error_ratio"] = (wv * (pred_t - R) ** 2).sum().item() / den
+        out["commutator_vs_residual_ratio"] = (wv * (true_t - R) ** 2).sum().item() / den
+        log(f"a priori residual error ratio {out['residual_error_ratio']:.4f} "
+            f"(exact commutator: {out['commutator_vs_residual_ratio']:.4f})")
+    return out
 
 
 TERMS = {"stress": range(0, 6), "heat": range(6, 9), "emf": range(9, 12)}
@@ -174,12 +285,14 @@ TERMS = {"stress": range(0, 6), "heat": range(6, 9), "emf": range(9, 12)}
 
 def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
     """A coarse FP32 run from the judge's filtered start over the window; with
-    net, the closure is attached with only the named term groups applied."""
+    net, the closure is attached with only the named term groups applied,
+    scaled by the gain after '@' (terms "stress+heat@0.5")."""
     g = mhd3d.GpuSim(judge["coarse_setup"], mode=mhd3d.MODE_FP32)
     g.upload(judge["start"])
     if net is not None:
+        terms, _, gain = terms.partition("@")
         keep = net.out_scale
-        sc = net.out_scale.clone()
+        sc = net.out_scale.clone() * (float(gain) if gain else 1.0)
         for name, idx in TERMS.items():
             if name not in terms.split("+"):
                 sc[list(idx)] = 0.0
@@ -215,17 +328,24 @@ def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
     return out
 
 
-def save_case(path, net, judge, tr, apri):
-    """The trained network and what the coarse runs are judged on."""
+WINDOW_KEYS = ("t0", "t1", "steps", "wall", "spin_steps", "dt_mean", "umach_max")
+
+
+def save_case(path, net, judge, tr, apri, val=None):
+    """The trained network and what the coarse runs are judged on (and, with
+    val, the training run's window for choosing a gain)."""
     d = {f"start_{f}": a for f, a in judge["start"].items() if a is not None}
+    if val is not None:
+        d.update({f"val_start_{f}": a for f, a in val["start"].items() if a is not None})
+        d["val_profiles"] = val["profiles"]
+        d["val_meta"] = np.array(json.dumps({k: val[k] for k in WINDOW_KEYS}))
     for li in range(len(closure.LAYERS)):
         d[f"w{li}"] = net.w[li].cpu().numpy()
         d[f"b{li}"] = net.b[li].cpu().numpy()
     d["in_scale"] = net.in_scale.cpu().numpy()
     d["out_scale"] = net.out_scale.cpu().numpy()
     d["profiles"] = judge["profiles"]
-    d["meta"] = np.array(json.dumps({k: judge[k] for k in ("t0", "t1", "steps", "wall", "spin_steps", "dt_mean",
-                                                            "umach_max")} | {"train": tr, "a_priori": apri}))
+    d["meta"] = np.array(json.dumps({k: judge[k] for k in WINDOW_KEYS} | {"train": tr, "a_priori": apri}))
     np.savez(path, **d)
 
 
@@ -243,9 +363,16 @@ def load_case(path, args):
     fnx, fny, fnz = args.fine
     cs = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args, args.judge_seed))
     start = {f: (z[f"start_{f}"] if f"start_{f}" in z else None) for f in mhd3d.FIELDS}
-    judge = {k: meta[k] for k in ("t0", "t1", "steps", "wall", "spin_steps", "dt_mean", "umach_max")}
+    judge = {k: meta[k] for k in WINDOW_KEYS}
     judge.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
-    return net, judge, meta["train"], meta["a_priori"]
+    val = None
+    if "val_profiles" in z:
+        val = json.loads(str(z["val_meta"]))
+        val["start"] = {f: (z[f"val_start_{f}"] if f"val_start_{f}" in z else None) for f in mhd3d.FIELDS}
+        val["profiles"] = z["val_profiles"]
+        val["coarse_setup"] = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args,
+                                                      args.train_seed))
+    return net, judge, meta["train"], meta["a_priori"], val
 
 
 def rel_errors(got, ref):
@@ -268,11 +395,18 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--trip", type=float, default=1.0)
+    ap.add_argument("--resid-steps", type=int, default=0,
+                    help="fine steps between the two filtered states of a residual target; 0: commutator only")
+    ap.add_argument("--resid-iters", type=int, default=3000)
+    ap.add_argument("--resid-lr", type=float, default=1e-3)
     ap.add_argument("--train-seed", type=int, default=101)
     ap.add_argument("--judge-seed", type=int, default=202)
     ap.add_argument("--net-seed", type=int, default=7)
     ap.add_argument("--variants", default="stress+heat+emf",
                     help="comma-separated closure runs, each a '+'-joined set of stress, heat, emf")
+    ap.add_argument("--gains", default=None,
+                    help="comma-separated closure gains tried on the training run's window; the best is judged")
+    ap.add_argument("--gain-terms", default="stress+heat+emf")
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the trained network and the judge run's window (.npz)")
     ap.add_argument("--load", default=None, help="skip the fine runs and training: read a --save file")
@@ -281,18 +415,42 @@ def main(argv=None):
     def log(msg):
         print(msg, file=sys.stderr, flush=True)
 
+    val = None
     if args.load:
-        net, judge, tr, apri = load_case(args.load, args)
+        net, judge, tr, apri, val = load_case(args.load, args)
     else:
         trainer = fine_phase(args, args.train_seed, True, log)
-        net, tr = train(trainer["pairs"], args, log)
-        del trainer
+        net, tr, data = train(trainer["pairs"], args, log)
+        val = {k: trainer[k] for k in WINDOW_KEYS + ("start", "profiles", "coarse_setup")}
+        w = None
+        if args.resid_steps:
+            tr["residual"], w = train_residual(net, data, trainer["resid"], trainer["pc"], args, log)
+        del trainer, data
         judge = fine_phase(args, args.judge_seed, False, log)
+        judge["resid_w"] = w
         apri = a_priori(net, judge, log)
         if args.save:
-            save_case(args.save, net, judge, tr, apri)
+            save_case(args.save, net, judge, tr, apri, val)
+    chosen = None
+    if args.gains and val is not None:
+        # the gain is chosen on the training run's own window, never on the judge's
+        scores = {}
+        for gv in args.gains.split(","):
+            run = coarse_phase(val, net, args, log, f"validate@{gv}", f"{args.gain_terms}@{gv}")
+            err = rel_errors(run["profiles"], val["profiles"])
+            scores[gv] = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
+            log(f"gain {gv}: status {run['status']} mean(ke, fconv, me) error {scores[gv]}")
+        ok = {k: v for k, v in scores.items() if v is not None}
+        plain_val = rel_errors(coarse_phase(val, None, args, log, "validate plain")["profiles"], val["profiles"])
+        chosen = min(ok, key=ok.get) if ok else None
+        tr["gain_scores"] = scores
+        tr["gain_plain_score"] = float(np.mean([plain_val[n] for n in ("ke", "fconv", "me")]))
+        tr["gain_chosen"] = chosen
     runs = [("plain", coarse_phase(judge, None, args, log, "plain"))]
-    for v in args.variants.split(","):
+    variants = args.variants.split(",") if args.variants else []
+    if chosen is not None:
+        variants.append(f"{args.gain_terms}@{chosen}")
+    for v in variants:
         runs.append(("closure" if v == "stress+heat+emf" else f"closure[{v}]",
                      coarse_phase(judge, net, args, log, f"closure[{v}]", v)))
     ref = judge["profiles"]
@@ -301,7 +459,7 @@ def main(argv=None):
         "window": [judge["t0"], judge["t1"]],
         "fine_window": {"steps": judge["steps"], "wall_s": judge["wall"], "dt_mean": judge["dt_mean"],
                         "spin_steps": judge["spin_steps"], "umach_max": judge["umach_max"]},
-        "train": tr, "a_priori_tendency_error_ratio": apri,
+        "train": tr, "a_priori": apri,
     }
     for name, run in runs:
         d = {k: v for k, v in run.items() if k != "profiles"}

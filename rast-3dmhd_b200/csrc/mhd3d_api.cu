@@ -551,6 +551,91 @@ __global__ void k_tendency(UView v, const float* __restrict__ pred, const float*
     }
 }
 
+// Adjoint of k_tendency's linear map pred -> tendencies: for output g
+// [7][nvox] (the loss gradient of each tendency) writes d loss / d pred as
+// BF16 [nvox][16] (channels 12..15 zero), the last layer's output gradient.
+// A term s * (P[n+1] - P[n-1]) * a[n] of tendency f at cell n hands
+// s * (a[m-1] g[m-1] - a[m+1] g[m+1]) to P[m]; TT's terms carry 1/RO of
+// cell n; the first and last z planes have no tendency.
+__global__ void k_tendency_adj(UView v, const float* __restrict__ g, const float* __restrict__ osc,
+                               const double* __restrict__ fax, const double* __restrict__ fay,
+                               const double* __restrict__ faz, int npx, int npy, int npz, size_t fstride,
+                               __nv_bfloat16* __restrict__ dpred)
+{
+    // (field, direction, sign) of each output channel, as k_tendency uses them
+    constexpr int NT[12] = {1, 1, 1, 2, 2, 2, 1, 1, 1, 2, 2, 2};
+    constexpr int TF[12][2] = {{0, 0}, {1, 0}, {2, 0}, {0, 1}, {0, 2}, {1, 2},
+                               {3, 0}, {3, 0}, {3, 0}, {5, 6}, {6, 4}, {4, 5}};
+    constexpr int TD[12][2] = {{0, 0}, {1, 0}, {2, 0}, {1, 0}, {2, 0}, {2, 1},
+                               {0, 0}, {1, 0}, {2, 0}, {2, 1}, {0, 2}, {1, 0}};
+    constexpr float TS[12][2] = {{-1, 0}, {-1, 0}, {-1, 0}, {-1, -1}, {-1, -1}, {-1, -1},
+                                 {-1, 0}, {-1, 0}, {-1, 0}, {1, -1}, {1, -1}, {1, -1}};
+    const size_t n = (size_t)npx * npy * npz;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % npx), j = (int)((q / npx) % npy), k = (int)(q / ((size_t)npx * npy));
+        // weighted gradient of field f at the neighbour one cell along d (side -1 or +1)
+        auto H = [&](int f, int d, int side) -> double {
+            int ii = i, jj = j, kk = k;
+            double a;
+            if (d == 0) {
+                ii = i + side;
+                ii = ii < 0 ? npx - 1 : (ii == npx ? 0 : ii);
+                a = fax[ii + 1];
+            } else if (d == 1) {
+                jj = j + side;
+                jj = jj < 0 ? npy - 1 : (jj == npy ? 0 : jj);
+                a = fay[jj + 1];
+            } else {
+                kk = k + side;
+                if (kk < 1 || kk > npz - 2) return 0.0;
+                a = faz[kk + 1];
+            }
+            if (d < 2 && (kk < 1 || kk > npz - 2)) return 0.0;
+            double h = (double)g[f * fstride + ((size_t)kk * npy + jj) * npx + ii] * a;
+            if (f == 3) h /= uget(v, F_RO, ii + 1, jj + 1, kk + 1);
+            return h;
+        };
+        __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            double acc = 0.0;
+            for (int t = 0; t < NT[c]; ++t)
+                acc += TS[c][t] * (H(TF[c][t], TD[c][t], -1) - H(TF[c][t], TD[c][t], 1));
+            o[c] = __float2bfloat16_rn((float)(acc * osc[c]));
+        }
+#pragma unroll
+        for (int c = 12; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+        uint4* dst = reinterpret_cast<uint4*>(dpred + q * 16);
+        dst[0] = reinterpret_cast<const uint4*>(o)[0];
+        dst[1] = reinterpret_cast<const uint4*>(o)[1];
+    }
+}
+
+// Weighted mean-square loss of the 7 tendencies against a target and its
+// gradient: loss += sum_f w_f sum_q (t - r)^2 / (7 nvox), g = d loss / d t.
+__global__ void __launch_bounds__(256) k_tendency_loss(const float* __restrict__ t, const float* __restrict__ r,
+                                                       const float* __restrict__ w, size_t nvox,
+                                                       float* __restrict__ g, double* __restrict__ loss)
+{
+    __shared__ double red[256];
+    const double nrm = 1.0 / ((double)nvox * 7.0);
+    double acc = 0.0;
+    const size_t n = nvox * 7;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const double wf = w[q / nvox] * nrm;
+        const double d = (double)t[q] - (double)r[q];
+        acc += wf * d * d;
+        g[q] = (float)(2.0 * wf * d);
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s2 = 128; s2 > 0; s2 >>= 1) {
+        if ((int)threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, red[0]);
+}
+
 __global__ void k_trip_count(int* flag)
 {
     flag[1] += flag[0] ? 1 : 0;
@@ -1957,6 +2042,32 @@ int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_sca
     k_tendency<<<grid_for(nv), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         uview(h, h->cur), pred, out_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy, npz, trip, out, nv,
         (size_t)npx * npy, (size_t)npx, flag);
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_tendency_adjoint(void* handle, const float* g, const float* out_scale, void* dpred, void* stream)
+{
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !g || !out_scale || !dpred) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    CK(cudaStreamSynchronize(h->st));
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t nv = (size_t)npx * npy * npz;
+    k_tendency_adj<<<grid_for(nv), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        uview(h, h->cur), g, out_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy, npz, nv,
+        static_cast<__nv_bfloat16*>(dpred));
+    CK(cudaGetLastError());
+    return MHD3D_OK;
+}
+
+int mhd3d_closure_tendency_loss(const float* tend, const float* target, const float* weight, int64_t nvox, float* g,
+                                double* loss, void* stream)
+{
+    if (!tend || !target || !weight || nvox <= 0 || !g || !loss) return MHD3D_ERR_ARG;
+    k_tendency_loss<<<grid_for((size_t)nvox * 7), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        tend, target, weight, (size_t)nvox, g, loss);
     CK(cudaGetLastError());
     return MHD3D_OK;
 }

@@ -130,6 +130,8 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_closure_loss.argtypes = [vp, vp, C.c_int64, vp, vp, vp]
     lib.mhd3d_adam.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, i32, vp, vp]
     lib.mhd3d_closure_tendency.argtypes = [vp, vp, vp, vp, vp, C.c_float, vp]
+    lib.mhd3d_closure_tendency_loss.argtypes = [vp, vp, vp, C.c_int64, vp, vp, vp]
+    lib.mhd3d_closure_tendency_adjoint.argtypes = [vp, vp, vp, vp, vp]
     lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_double)]
     lib.mhd3d_version.restype = C.c_char_p

@@ -31,3 +31,24 @@ def test_periodic_and_wall_padding():
     w2[0, 13 + 1] = 1.0   # tap (+1,0,0): out[z,y,x] = x[z,y,x+1]
     out2 = conv3d_fwd(x, w2)[..., 0]
     assert out2[0, 0, 7] == 1.0 and out2.sum() == 1.0
+
+
+def test_tendency_adjoint_identity():
+    from closure_oracle import tendency_adj, tendency_fwd
+    rng = np.random.default_rng(3)
+    nz, ny, nx = 6, 5, 8
+    p = rng.standard_normal((nz, ny, nx, 16))
+    osc = rng.uniform(0.5, 2.0, 12)
+    ax, ay, az = rng.uniform(1, 2, nx), rng.uniform(1, 2, ny), rng.uniform(1, 2, nz)
+    ro = rng.uniform(0.5, 1.5, (nz, ny, nx))
+    g = rng.standard_normal((7, nz, ny, nx))
+    t = tendency_fwd(p, osc, ax, ay, az, ro)
+    assert not t[:, 0].any() and not t[:, -1].any()
+    d = tendency_adj(g, osc, ax, ay, az, ro)
+    assert not d[..., 12:].any()
+    assert np.isclose(np.sum(t * g), np.sum(p * d), rtol=1e-12)
+    # one stress component: RU's tendency is minus the x difference of tau_xx
+    q = np.zeros_like(p)
+    q[2, 2, 3, 0] = 1.0
+    t = tendency_fwd(q, np.ones(12), np.ones(nx), np.ones(ny), np.ones(nz), np.ones((nz, ny, nx)))
+    assert t[0, 2, 2, 2] == -1.0 and t[0, 2, 2, 4] == 1.0 and np.abs(t).sum() == 2.0

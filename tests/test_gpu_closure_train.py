@@ -7,7 +7,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from closure_oracle import conv3d_dw, conv3d_dx, conv3d_fwd
+from closure_oracle import conv3d_dw, conv3d_dx, conv3d_fwd, tendency_adj, tendency_fwd
 from test_gpu_parity import _gpu_or_skip
 
 pytestmark = pytest.mark.gpu
@@ -123,6 +123,66 @@ def test_network_gradients_layer_by_layer(mhd3d):
         assert np.abs(dxf.double().cpu().numpy() - rdx).max() <= 2e-5 * np.abs(rdx).max()
         dy = dxf.to(torch.bfloat16)
     assert int(net.err.item()) == 0
+
+
+def test_tendency_loss_and_adjoint(mhd3d):
+    """The closure tendencies, their weighted loss and the adjoint that turns
+    the loss gradient into the last layer's dy, against the numpy checker."""
+    _gpu_or_skip(mhd3d)
+    torch = pytest.importorskip("torch")
+    from test_gpu_parity import _random_state
+    lib = mhd3d.gpu_lib()
+    setup = mhd3d.make_setup(mhd3d.convection_config(32, 12, 10, ra=1e5, ta=1e4, seed=4))
+    st = _random_state(mhd3d, setup, seed=5, amp=0.05)
+    g = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    g.upload(st)
+    p = g.params
+    nz, ny, nx = p.npz, p.npy, p.npx
+    rng = np.random.default_rng(2)
+    pred = torch.tensor(rng.standard_normal((nz, ny, nx, 16)), dtype=torch.float32, device="cuda")
+    osc = torch.tensor(rng.uniform(0.5, 2.0, 12), dtype=torch.float32, device="cuda")
+    ax = p.hx * setup.grid["dxxdx"][1:-1]
+    ay = p.hy * setup.grid["dyydy"][1:-1]
+    az = p.hz * setup.grid["dzzdz"][1:-1]
+    ro = np.transpose(st["ro"][1:-1, 1:-1, 1:-1], (2, 1, 0))
+    s = torch.cuda.current_stream().cuda_stream
+    tend = torch.empty((7, nz, ny, nx), dtype=torch.float32, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.mhd3d_closure_tendency(g.h, _p(pred), _p(osc), _p(tend), _p(flag), C.c_float(1e30), C.c_void_p(s)) == 0
+    torch.cuda.synchronize()
+    P, O = pred.double().cpu().numpy(), osc.double().cpu().numpy()
+    ref = tendency_fwd(P, O, ax, ay, az, ro)
+    assert np.abs(tend.double().cpu().numpy() - ref).max() <= 1e-5 * np.abs(ref).max()
+    # loss and gradient against a target
+    tgt = torch.tensor(rng.standard_normal((7, nz, ny, nx)), dtype=torch.float32, device="cuda")
+    w = torch.tensor(rng.uniform(0.5, 2.0, 7), dtype=torch.float32, device="cuda")
+    gr = torch.empty_like(tend)
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert lib.mhd3d_closure_tendency_loss(_p(tend), _p(tgt), _p(w), nz * ny * nx, _p(gr), _p(loss), C.c_void_p(s)) == 0
+    torch.cuda.synchronize()
+    T, R, W = tend.double().cpu().numpy(), tgt.double().cpu().numpy(), w.double().cpu().numpy()
+    n = 7 * nz * ny * nx
+    d = T - R
+    assert abs(loss.item() - (W[:, None, None, None] * d * d).sum() / n) <= 1e-9 * loss.item()
+    G = gr.double().cpu().numpy()
+    assert np.abs(G - 2 * W[:, None, None, None] * d / n).max() <= 1e-6 * np.abs(G).max()
+    # adjoint (BF16 output)
+    dy = torch.empty((nz, ny, nx, 16), dtype=torch.bfloat16, device="cuda")
+    assert lib.mhd3d_closure_tendency_adjoint(g.h, _p(gr), _p(osc), _p(dy), C.c_void_p(s)) == 0
+    torch.cuda.synchronize()
+    radj = tendency_adj(G, O, ax, ay, az, ro)
+    got = dy.double().cpu().numpy()
+    assert np.abs(got - radj).max() <= 8e-3 * np.abs(radj).max()
+    assert not got[..., 12:].any()
+    # the same through the training helper
+    import closure
+    net = closure.ClosureNet(seed=0)
+    net.out_scale = osc
+    l2, dy2 = net.tendency_loss_and_grad(g, pred, tgt, w, s)
+    torch.cuda.synchronize()
+    assert abs(l2.item() - loss.item()) <= 1e-12 * loss.item()
+    assert torch.equal(dy2, dy)
+    g.close()
 
 
 def _coarse_setup(mhd3d):
