@@ -282,7 +282,8 @@ int mhd3d_ensemble_set_stream(void* ens, void* stream);
  * arrays are device pointers; activations are channels-last BF16
  * [nz][ny][nx][C] (periodic in x and y, zero outside in z), weights BF16
  * [cout][27*cin] with k = tap*cin + ci, tap = (dx+1) + 3*(dy+1) + 9*(dz+1).
- * nx must be a multiple of 128 or divide 128.  Supported (cin, cout): (16,32), (32,32),
+ * nx must be a multiple of 128 or divide 128; every array is 16-byte aligned.
+ * Supported (cin, cout): (16,32), (32,32),
  * (32,16).  Work is enqueued on stream; err (device int) is set non-zero if
  * a bounded wait of the tensor-core pipeline gave up.
  *
@@ -322,8 +323,8 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
  * error of pred [v][16] against target [v][12] to *loss and writes its
  * gradient dy [v][16] BF16.  mhd3d_adam: one Adam step on FP32 parameters
  * (step number t), optional BF16 copy.  mhd3d_closure_tendency: the
- * tendencies of pred for a handle's state, out[f][k][j][i] (f = RU, RV, RW,
- * TT, BX, BY, BZ); *flag set when the indicator trips.
+ * tendencies of pred (16-byte aligned) for a handle's state, out[f][k][j][i]
+ * (f = RU, RV, RW, TT, BX, BY, BZ); *flag set when the indicator trips.
  */
 int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void* w2, const float* b2, const void* w3,
                       const float* b3, const float* in_scale, const float* out_scale, float trip);

@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/mhd3d.h"
 #include "ring.cuh"
@@ -39,7 +40,9 @@
 namespace mhd3d {
 namespace clo {
 
-constexpr int CT = 128;            // threads of a convolution CTA (4 warps: TMEM lanes 0..127)
+constexpr int NLW = 4;             // loader warps of a convolution CTA
+constexpr int CT = 32 * (4 + NLW + 1);   // threads: 4 epilogue warps (TMEM lanes 0..127), loaders, MMA
+constexpr int RING = 4;            // input rows held in the ring: the loaders run up to three steps ahead
 constexpr int MT = 128;            // output voxels per tile: one 128-point x segment
 constexpr int BX = MT + 2;         // input block: x with halo
 constexpr int VB = BX * 3 * 3;     // voxels of the input block (y, z halos)
@@ -140,19 +143,22 @@ __device__ __forceinline__ void load_block_async(unsigned char* sx, const __nv_b
                      : "memory");
     }
 }
-// Ring of y rows for the convolution: [chunk][slot 0..3][z plane 0..2][BX voxels]
-// of 16-byte rows; row yr (unwrapped) lives in slot yr & 3.
-constexpr int RSEG = 4 * 3 * BX;   // voxel rows of one chunk of the ring
+// Ring of input rows for the convolution: [chunk][slot 0..RING-1][z plane 0..2]
+// [BXP] of 16-byte rows, voxel xi (x0-1+xi) at row XR0+xi, so that the 128
+// interior voxels start on a 128-byte boundary (a TMA destination); step s of
+// a CTA keeps its input row in slot s % RING.
+constexpr int XR0 = 7;
+constexpr int BXP = 144;              // XR0 + BX rounded up to 8 rows
+constexpr int RSEG = RING * 3 * BXP;  // voxel rows of one chunk of the ring
 template <int CIN, int NTH>
 __device__ __forceinline__ void load_row_async(unsigned char* ring, const __nv_bfloat16* __restrict__ x, int x0,
-                                               int yr, int z, int nx, int ny, int nz)
+                                               int yr, int z, int nx, int ny, int nz, int tix, int slot)
 {
     constexpr int NC = CIN / 8;
-    const int slot = yr & 3;
     int gy = yr % ny;
     gy = gy < 0 ? gy + ny : gy;
     const uint32_t sbase = smem_u32(ring);
-    for (int q = threadIdx.x; q < 3 * BX * NC; q += NTH) {
+    for (int q = tix; q < 3 * BX * NC; q += NTH) {
         const int c = q / (3 * BX), r = q % (3 * BX);
         const int zi = r / BX, xi = r % BX;
         int gx = x0 - 1 + xi;
@@ -162,7 +168,7 @@ __device__ __forceinline__ void load_row_async(unsigned char* ring, const __nv_b
         const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
         gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
         const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8;
-        const uint32_t dst = sbase + (uint32_t)((c * RSEG + (slot * 3 + zi) * BX + xi) * 16);
+        const uint32_t dst = sbase + (uint32_t)((c * RSEG + (slot * 3 + zi) * BXP + XR0 + xi) * 16);
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(nbytes) : "memory");
     }
 }
@@ -171,112 +177,380 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// The input row of a step by TMA (x segments of 128 voxels, nx a multiple of
+// 128): one 5-D box (8 channels, 1 chunk, 128 x, 1 y, 1 z) per chunk and z
+// plane into the ring's interior rows, zeros outside z (out-of-range box);
+// the two periodic x halo voxels by cp.async from the calling warp.  The
+// TMA bytes complete on bar (after the caller's expect_tx); each lane's
+// copies are signalled by the caller's cp.async.mbarrier.arrive.
+template <int CIN>
+__device__ __forceinline__ void load_row_tma(unsigned char* ring, const CUtensorMap* map, unsigned long long* bar,
+                                             const __nv_bfloat16* __restrict__ x, int x0, int yr, int z, int nx,
+                                             int ny, int nz, int lane, int slot)
+{
+    constexpr int NC = CIN / 8;
+    int gy = yr % ny;
+    gy = gy < 0 ? gy + ny : gy;
+    const uint32_t sbase = smem_u32(ring);
+    if (lane == 0) {
+        for (int c = 0; c < NC; ++c)
+            for (int zi = 0; zi < 3; ++zi) {
+                const uint32_t dst = sbase + (uint32_t)((c * RSEG + (slot * 3 + zi) * BXP + XR0 + 1) * 16);
+                asm volatile(
+                    "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3, %4, %5, %6}], [%7];" ::"r"(dst),
+                    "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(c), "r"(x0), "r"(gy), "r"(z - 1 + zi),
+                    "r"(smem_u32(bar))
+                    : "memory");
+            }
+    }
+    for (int q = lane; q < 2 * NC * 3; q += 32) {
+        const int side = q & 1, c = (q >> 1) % NC, zi = (q >> 1) / NC;
+        const int xi = side ? BX - 1 : 0;
+        int gx = x0 - 1 + xi;
+        gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        int gz = z - 1 + zi;
+        const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
+        gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
+        const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8;
+        const uint32_t dst = sbase + (uint32_t)((c * RSEG + (slot * 3 + zi) * BXP + XR0 + xi) * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(nbytes) : "memory");
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait without sleeping between polls: mbarrier.try_wait itself
+// suspends the thread for a while, and the pipeline's hand-offs between warp
+// roles are on the critical path; false when it gave up
+__device__ __forceinline__ bool mbar_wait_fast(unsigned long long* bar, unsigned parity)
+{
+    for (long it = 0; it < WAIT_LIMIT; ++it)
+        if (mbar_test(bar, parity)) return true;
+    return false;
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_st_zero(uint32_t taddr);
+
+template <>
+__device__ __forceinline__ void tmem_st_zero<16>(uint32_t taddr)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+template <>
+__device__ __forceinline__ void tmem_st_zero<32>(uint32_t taddr)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// The steps of a CTA.  Its range of output rows is split into two halves,
+// each walked as runs along y within one (x segment, z) column; a run of
+// output rows ya..yb takes input rows ya-1..yb+1, one step each.  The steps of
+// the two halves alternate (then the longer half finishes alone), so that two
+// accumulator sets take turns on the tensor cores.  f(s, X, k, x0, z, r,
+// first, emit) for every step s in order: X the half (accumulator set), k the
+// step's index within its half, r the unwrapped input row, first the run's
+// first step, emit whether output row r-1 is in the run; f returns false to
+// stop.
+constexpr bool TWO_SETS = false;   // alternate two halves of the range (measured slower: more runs)
+
+struct RunCursor {
+    int t, t_end, ny, nz, ya, yb, z, x0, r;
+    bool live;
+    __device__ void start_run()
+    {
+        live = t < t_end;
+        if (!live) return;
+        ya = t % ny;
+        z = (t / ny) % nz;
+        x0 = (t / (ny * nz)) * MT;
+        const int run = (t_end - t) < (ny - ya) ? (t_end - t) : (ny - ya);
+        yb = ya + run - 1;
+        r = ya - 1;
+        t += run;
+    }
+    __device__ void next()
+    {
+        if (++r > yb + 1) start_run();
+    }
+};
+
+template <class F>
+__device__ __forceinline__ void for_steps(int t_begin, int t_end, int ny, int nz, F f)
+{
+    const int t_mid = TWO_SETS ? t_begin + (t_end - t_begin) / 2 : t_begin;
+    // a: the half whose turn it is (the second, longer half leads); swapped
+    // rather than indexed so the cursors stay in registers
+    RunCursor a, b;
+    a.t = t_mid;
+    a.t_end = t_end;
+    b.t = t_begin;
+    b.t_end = t_mid;
+    a.ny = b.ny = ny;
+    a.nz = b.nz = nz;
+    a.start_run();
+    b.start_run();
+    int xa = 1, xb = 0, ka = 0, kb = 0;
+    auto swap_ab = [&]() {
+        const RunCursor tc = a;
+        a = b;
+        b = tc;
+        const int tx = xa;
+        xa = xb;
+        xb = tx;
+        const int tk = ka;
+        ka = kb;
+        kb = tk;
+    };
+    for (int s = 0; a.live || b.live; ++s) {
+        if (!a.live) swap_ab();
+        if (!f(s, xa, ka, a.x0, a.z, a.r, a.r == a.ya - 1, a.r - 1 >= a.ya && a.r - 1 <= a.yb)) return;
+        a.next();
+        ++ka;
+        if (b.live) swap_ab();
+    }
+}
+
 template <int CIN, int COUT>
 struct ConvLay {
     static constexpr int K = 27 * CIN;
-    static constexpr size_t W_B = (size_t)COUT * K * 2;
+    static constexpr int KB = 9 * CIN;          // K of one y-tap block: (dz, dx, ci)
+    static constexpr int NW = 3 * COUT;         // N of an MMA: three output rows
+    static constexpr uint32_t SET = NW <= 64 ? 64 : 128;   // TMEM columns of one accumulator set
+    static constexpr uint32_t NCOL = 2 * SET;
+    static constexpr size_t W_B = (size_t)5 * COUT * KB * 2;   // y-tap blocks 2, 1, 0, 2, 1
     static constexpr size_t X_OFF = (W_B + 127) / 128 * 128;
-    static constexpr size_t X_B = ((size_t)CIN * RSEG * 2 + 127) / 128 * 128;  // ring of four y rows
+    static constexpr size_t X_B = ((size_t)CIN * RSEG * 2 + 127) / 128 * 128;  // ring of RING input rows
     static constexpr size_t BAR_OFF = X_OFF + X_B;
-    static constexpr size_t BYTES = BAR_OFF + 16 + 128;
+    // barriers: ready[4], mmadone[4], accfull[2], accempty[2]; then the TMEM
+    // address, the abort flag and the last committed step
+    static constexpr size_t BYTES = BAR_OFF + 12 * 8 + 16 + 128;
 };
 
 // Y = act(conv(X, W) + bias) [* (mask > 0)], persistent over (x segment, y, z) tiles.
 // w: [COUT][27*CIN] BF16, k = tap*CIN + ci with tap = dx+1 + 3*(dy+1) + 9*(dz+1).
+//
+// One MMA serves three output rows: an input row r (one of the CTA's steps)
+// contributes to output rows r+1, r, r-1 through the weights of y-taps 0, 1,
+// 2.  Three accumulators of COUT columns sit side by side in TMEM, output row
+// y in slot y mod 3, and the B operand stacks the y-tap blocks in the slot
+// order, which rotates with r mod 3: the weights are kept as the y-tap blocks
+// 2, 1, 0, 2, 1 and each step reads the window of three starting at
+// (1 - r) mod 3.  Per input row the MMAs are 9 * CIN/16 of N = 3*COUT
+// (instead of 27 * CIN/16 of N = COUT per output row), so each input tile
+// is read from shared memory a third as often.  After step r, output row r-1
+// is complete: the epilogue reads its slot, zeroes it for output row r+2 and
+// stores.  The first MMA of a run starts all three slots from zero.
+//
+// Warp roles, pipelined over the CTA's steps s (ready and mmadone by s & 3):
+//   warps 4..4+NLW-1 (loaders): cp.async of the step's input row (three z
+//     planes, periodic in x and y, zeros outside z) into ring slot s % RING;
+//     each thread's copies arrive on ready(s) as they land
+//     (cp.async.mbarrier.arrive), and the slot is reused once the MMAs of
+//     step s - RING have completed (mmadone).
+//   warp 4+NLW, lane 0 (MMA): waits ready(s) and the release of its set's
+//     previous step (accempty), issues the step's MMAs into that set,
+//     commits to the set's accfull and to mmadone(s).  While one set's
+//     finished slot is read out, the MMAs of the other set's step run.
+//   warps 0-3 (epilogue): wait accfull of the step's set, read and zero the
+//     finished slot (TMEM lanes 32*warp..), release it (accempty) and store.
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restrict__ x,
+__global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtensorMap xmap, int use_tma,
+                                                  const __nv_bfloat16* __restrict__ x,
                                                   const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
                                                   const __nv_bfloat16* __restrict__ mask, int relu,
                                                   __nv_bfloat16* __restrict__ y, float* __restrict__ yf, int nx, int ny,
                                                   int nz, int* err)
 {
     using L = ConvLay<CIN, COUT>;
-    constexpr int K = L::K;
+    constexpr int K = L::K, KB = L::KB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     unsigned char* const sw = sb;
     unsigned char* const sx = sb + L::X_OFF;
-    unsigned long long* const bar = reinterpret_cast<unsigned long long*>(sb + L::BAR_OFF);
-    uint32_t* const tslot = reinterpret_cast<uint32_t*>(sb + L::BAR_OFF + 8);
+    unsigned long long* const bars = reinterpret_cast<unsigned long long*>(sb + L::BAR_OFF);
+    unsigned long long* const ready = bars;
+    unsigned long long* const mmadone = bars + 4;
+    unsigned long long* const accfull = bars + 8;    // per accumulator set
+    unsigned long long* const accempty = bars + 10;  // per accumulator set
+    uint32_t* const tslot = reinterpret_cast<uint32_t*>(sb + L::BAR_OFF + 96);
+    volatile int* const abort_flag = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 100);
+    volatile int* const last_commit = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 104);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // weights -> canonical K-major layout: (n, k) at ((n/8)*(K/8) + k/8)*128 + (n%8)*16 + (k%8)*2
-    for (int q = tid; q < COUT * (K / 8); q += CT) {
-        const int n = q / (K / 8), kc = q % (K / 8);
-        const uint4 v = *reinterpret_cast<const uint4*>(w + (size_t)n * K + kc * 8);
-        *reinterpret_cast<uint4*>(sw + ((size_t)(n >> 3) * (K / 8) + kc) * 128 + (n & 7) * 16) = v;
+    // weights -> y-tap blocks 2,1,0,2,1 of [COUT][KB], k' = (dz*3 + dx)*CIN + ci, in
+    // the canonical K-major layout: row n', k' at ((n'/8)*(KB/8) + k'/8)*128 + (n'%8)*16 + (k'%8)*2
+    {
+        // eight loads in flight per thread before their stores
+        constexpr int NQ = 5 * COUT * (KB / 8), BATCH = 8;
+        for (int q0 = tid; q0 < NQ; q0 += CT * BATCH) {
+            uint4 v[BATCH];
+            int dst[BATCH];
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u) {
+                const int q = q0 + u * CT;
+                dst[u] = -1;
+                if (q < NQ) {
+                    const int blk = q / (COUT * (KB / 8)), rem = q % (COUT * (KB / 8));
+                    const int n = rem / (KB / 8), kc = rem % (KB / 8);
+                    const int dyi = blk == 2 ? 0 : (blk == 1 || blk == 4) ? 1 : 2;
+                    const int dzdx = (kc * 8) / CIN, ci = (kc * 8) % CIN, dzi = dzdx / 3, dxi = dzdx % 3;
+                    const int tap = dxi + 3 * dyi + 9 * dzi;
+                    v[u] = __ldg(reinterpret_cast<const uint4*>(w + (size_t)n * K + tap * CIN + ci));
+                    const int nr = blk * COUT + n;
+                    dst[u] = (int)(((nr >> 3) * (KB / 8) + kc) * 128 + (nr & 7) * 16);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BATCH; ++u)
+                if (dst[u] >= 0) *reinterpret_cast<uint4*>(sw + dst[u]) = v[u];
+        }
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(32u)
+                     "r"(L::NCOL)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(bar, 1);
+        for (int b = 0; b < 4; ++b) {
+            // TMA: the expect_tx arrival and one completion arrival per lane of
+            // the loader warp; cp.async only: one per loader thread
+            mbar_init(ready + b, use_tma ? 1 + 32 : 32 * NLW);
+            mbar_init(mmadone + b, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accfull + b, 1);
+            mbar_init(accempty + b, 4);
+        }
+        *abort_flag = 0;
+        *last_commit = -1;
         fence_mbar_init();
     }
+    fence_proxy_async();   // the weights, written by plain stores, are read by the tensor cores
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    // tiles in (segment, z, y) order with y fastest; each CTA takes one
-    // contiguous run, so consecutive tiles share two of their three y rows
+    // output rows in (segment, z, y) order with y fastest; each CTA takes one
+    // contiguous range, walked as runs along y
     const int nseg = (nx + MT - 1) / MT;
     const int ntile = nseg * ny * nz;
-    constexpr uint32_t IDESC = idesc_bf16(MT, COUT);
-    const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
     const int t_begin = (int)(((long)ntile * blockIdx.x) / gridDim.x);
     const int t_end = (int)(((long)ntile * (blockIdx.x + 1)) / gridDim.x);
-    auto tile_of = [&](int t, int& x0, int& yy, int& zz) {
-        yy = t % ny;
-        zz = (t / ny) % nz;
-        x0 = (t / (ny * nz)) * MT;
+    auto give_up = [&]() {
+        *abort_flag = 1;
+        atomicExch(err, 1);
     };
-    unsigned phase = 0;
-    bool failed = false;
-    for (int t = t_begin; t < t_end && !failed; ++t) {
-        int x0, yy, zz;
-        tile_of(t, x0, yy, zz);
-        const bool fresh = t == t_begin || yy == 0;   // a new (segment, z) run: rows y-1, y, y+1
-        if (fresh) {
-            for (int d = -1; d <= 1; ++d) load_row_async<CIN, CT>(sx, x, x0, yy + d, zz, nx, ny, nz);
-            cp_async_commit();
-        }
-        // the next tile's new row streams in while this tile is multiplied
-        if (t + 1 < t_end && yy + 1 < ny) load_row_async<CIN, CT>(sx, x, x0, yy + 2, zz, nx, ny, nz);
-        cp_async_commit();
-        cp_async_wait<1>();
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-            for (int tap = 0; tap < 27; ++tap) {
-                const int dxi = tap % 3, dyi = (tap / 3) % 3, dzi = tap / 9;
-                const int row = ((((yy + dyi - 1) & 3) * 3 + dzi) * BX + dxi);
-#pragma unroll
-                for (int kk = 0; kk < CIN / 16; ++kk) {
-                    const uint64_t da = smem_desc(sx_a + (uint32_t)((2 * kk) * RSEG + row) * 16u, RSEG * 16, 128);
-                    const uint64_t db = smem_desc(sw_a + (uint32_t)((tap * CIN + kk * 16) >> 3) * 128u, 128,
-                                                  (K / 8) * 128);
-                    umma_bf16(tmem, da, db, IDESC, (tap | kk) != 0 ? 1u : 0u);
-                }
+
+    if (use_tma && warp == 4) {
+        // one warp: the TMA boxes of the step's row and its two halo voxels
+        for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int x0, int zz, int r, bool, bool) {
+            if (*abort_flag) return false;
+            const int jw = s - RING;   // slot s % RING was last read by step s - RING
+            if (jw >= 0 && !mbar_wait_fast(mmadone + (jw & 3), (unsigned)(jw >> 2) & 1u)) {
+                give_up();
+                return false;
             }
-            umma_commit(bar);
+            unsigned long long* const bar = ready + (s & 3);
+            if (lane == 0) mbar_expect_tx(bar, (unsigned)(CIN / 8 * 3 * MT * 16));
+            load_row_tma<CIN>(sx, &xmap, bar, x, x0, r, zz, nx, ny, nz, lane, s % RING);
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+            return true;
+        });
+        cp_async_wait<0>();
+    } else if (!use_tma && warp >= 4 && warp < 4 + NLW) {
+        // each loader thread's copies of step s arrive on ready(s) when they
+        // land, so the loaders run ahead as far as the ring allows
+        const int tix = tid - 128;
+        for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int x0, int zz, int r, bool, bool) {
+            if (*abort_flag) return false;
+            // slot s % RING was last read by step s - RING
+            const int jw = s - RING;
+            if (jw >= 0 && !mbar_wait_fast(mmadone + (jw & 3), (unsigned)(jw >> 2) & 1u)) {
+                give_up();
+                return false;
+            }
+            load_row_async<CIN, 32 * NLW>(sx, x, x0, r, zz, nx, ny, nz, tix, s % RING);
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(ready + (s & 3)))
+                         : "memory");
+            return true;
+        });
+        cp_async_wait<0>();
+    } else if (warp == 4 + NLW) {
+        if (lane == 0) {
+            constexpr uint32_t IDESC = idesc_bf16(MT, L::NW);
+            const uint64_t da0 = smem_desc(smem_u32(sx), RSEG * 16, 128);
+            const uint64_t db0 = smem_desc(smem_u32(sw), 128, (KB / 8) * 128);
+            for_steps(t_begin, t_end, ny, nz, [&](int s, int X, int k, int, int, int r, bool first, bool) {
+                if (*abort_flag) return false;
+                if (!mbar_wait_fast(ready + (s & 3), (unsigned)(s >> 2) & 1u) ||
+                    (k > 0 && !mbar_wait_fast(accempty + X, (unsigned)(k - 1) & 1u))) {
+                    give_up();
+                    return false;
+                }
+                fence_proxy_async();   // the ring row, written by cp.async, is read by the tensor cores
+                tc_fence_after();
+                // window of y-tap blocks for slots 0, 1, 2: starts at (1 - r) mod 3
+                const uint32_t st = (uint32_t)(((1 - r) % 3 + 3) % 3);
+                const uint64_t dbs = db0 + (uint64_t)(st * (COUT / 8) * (KB / 8) * 8);
+                const uint32_t as = (uint32_t)((s % RING) * 3 * BXP + XR0);
+#pragma unroll
+                for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                    for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                        for (int kk = 0; kk < CIN / 16; ++kk) {
+                            const uint64_t da = da0 + (uint64_t)(as + (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
+                            const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
+                            umma_bf16(tmem + (uint32_t)X * L::SET, da, db, IDESC,
+                                      (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
+                        }
+                umma_commit(accfull + X);
+                umma_commit(mmadone + (s & 3));
+                *last_commit = s;
+                return true;
+            });
         }
-        if (!mbar_wait(bar, phase)) {
-            failed = true;
-            if (tid == 0) atomicExch(err, 1);
-        }
-        phase ^= 1u;
-        tc_fence_after();
-        if (!failed) {
+        __syncwarp();
+    } else if (warp < 4) {   // loader warps without work (TMA rows) take no role
+        for_steps(t_begin, t_end, ny, nz, [&](int, int X, int k, int x0, int zz, int r, bool, bool emit) {
+            if (*abort_flag) return false;
+            if (!mbar_wait_fast(accfull + X, (unsigned)k & 1u)) {
+                give_up();
+                return false;
+            }
+            tc_fence_after();
+            const int yo = r - 1;   // the output row this step completes
+            const uint32_t col = (uint32_t)X * L::SET + (uint32_t)((((yo % 3) + 3) % 3) * COUT);
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + col;
             float acc[COUT];
-            tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), acc);
+            if (emit) tmem_ld<COUT>(ta, acc);
+            tmem_st_zero<COUT>(ta);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(accempty + X);
+            if (!emit) return true;
             const int m = warp * 32 + lane;
             const bool own = x0 + m < nx;   // for nx < 128 the tile repeats the row's period
-            const size_t vox = ((size_t)zz * ny + yy) * nx + (own ? x0 + m : 0);
+            const size_t vox = ((size_t)zz * ny + yo) * nx + (own ? x0 + m : 0);
 #pragma unroll
             for (int n = 0; n < COUT; ++n) {
                 float o = acc[n] + (bias ? bias[n] : 0.f);
@@ -299,13 +573,21 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __nv_bfloat16* __restric
                     *reinterpret_cast<float4*>(yf + vox * COUT + n) =
                         make_float4(acc[n], acc[n + 1], acc[n + 2], acc[n + 3]);
             }
-        }
-        tc_fence_before();
-        __syncthreads();
+            return true;
+        });
     }
-    cp_async_wait<0>();
+    // every MMA has completed once the epilogue has seen its last accumulator;
+    // after an abort, wait (bounded) for the last issued step's MMAs before
+    // freeing TMEM
+    __syncthreads();
+    if (*abort_flag && tid == 0 && *last_commit >= 0) {
+        const int jl = *last_commit;
+        mbar_wait_fast(mmadone + (jl & 3), (unsigned)(jl >> 2) & 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
     tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::NCOL));
 }
 
 // dW[n][tap*CIN+ci] += sum_v dY[v][n] * X[v+tap][ci], db[n] += sum_v dY[v][n].
@@ -376,6 +658,29 @@ __global__ void k_wtranspose(const __nv_bfloat16* __restrict__ w, __nv_bfloat16*
     }
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 5-D tiled TMA map of a BF16 array, no swizzle, zeros outside
+cudaError_t encode_bf16_5d(CUtensorMap* map, void* base, const cuuint64_t dims[5], const cuuint64_t strides[4],
+                           const cuuint32_t box[5])
+{
+    static EncodeTiledFn enc = nullptr;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+            return cudaErrorInvalidValue;
+        enc = reinterpret_cast<EncodeTiledFn>(fn);
+    }
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 template <int CIN, int COUT>
 cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const void* mask, int relu, void* y,
                           float* yf, int nx, int ny, int nz, int* err, cudaStream_t st)
@@ -393,8 +698,19 @@ cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntile = ((nx + MT - 1) / MT) * ny * nz;
     const int grid = ntile < sms ? ntile : sms;
+    // rows of x segments of 128 by TMA: (8 channels, chunk, x, y, z) boxes
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    const int use_tma = nx % MT == 0 ? 1 : 0;
+    if (use_tma) {
+        const cuuint64_t dims[5] = {8, (cuuint64_t)CIN / 8, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        const cuuint64_t strides[4] = {16, (cuuint64_t)CIN * 2, (cuuint64_t)nx * CIN * 2,
+                                       (cuuint64_t)nx * ny * CIN * 2};
+        const cuuint32_t box[5] = {8, 1, (cuuint32_t)MT, 1, 1};
+        if (encode_bf16_5d(&map, const_cast<void*>(x), dims, strides, box) != cudaSuccess) return cudaErrorInvalidValue;
+    }
     k_conv3d<CIN, COUT><<<grid, CT, L::BYTES, st>>>(
-        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
+        map, use_tma, static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
         static_cast<const __nv_bfloat16*>(mask), relu, static_cast<__nv_bfloat16*>(y), yf, nx, ny, nz, err);
     return cudaGetLastError();
 }
@@ -425,6 +741,9 @@ cudaError_t launch_wgrad_t(const void* x, const void* dy, float* dw, float* db, 
 
 using namespace mhd3d::clo;
 
+// activations and weights move as 16-byte vectors
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 extern "C" {
 
 int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const float* bias, const void* mask,
@@ -432,6 +751,7 @@ int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const 
 {
     if (!x || !w || !err || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0 || (!y && !yf))
         return MHD3D_ERR_ARG;
+    if (!aligned16(x) || !aligned16(w) || !aligned16(mask) || !aligned16(y) || !aligned16(yf)) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (cin == 16 && cout == 32) e = launch_conv_t<16, 32>(x, w, bias, mask, relu, y, yf, nx, ny, nz, err, st);
@@ -445,6 +765,7 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
                        int32_t ny, int32_t nz, void* stream)
 {
     if (!x || !dy || !dw || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0) return MHD3D_ERR_ARG;
+    if (!aligned16(x) || !aligned16(dy)) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (cin == 16 && cout == 32) e = launch_wgrad_t<16, 32>(x, dy, dw, db, nx, ny, nz, st);

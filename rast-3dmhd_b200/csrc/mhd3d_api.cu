@@ -410,29 +410,42 @@ __global__ void k_fort_wrap(double* __restrict__ a, int nf, int npx, int npy, in
     }
 }
 
-// per-plane horizontal means of TT, RO, BY (network features)
-__global__ void __launch_bounds__(256) k_hmeans3(UView v, int npx, int npy, double* __restrict__ means, int npz,
-                                                 int lmag)
+// per-plane horizontal means of TT, RO, BY (network features): one CTA per
+// plane; the FP32 form sums the perturbations and adds the plane's background
+// once
+constexpr int HM_THREADS = 1024;
+__global__ void __launch_bounds__(HM_THREADS) k_hmeans3(UView v, int npx, int npy, double* __restrict__ means,
+                                                        int npz, int lmag)
 {
-    __shared__ double red[256];
-    const int k = blockIdx.x;
-    double st = 0, sr = 0, sb = 0;
-    for (int q = threadIdx.x; q < npx * npy; q += 256) {
+    __shared__ double red[3][HM_THREADS / 32];
+    const int k = blockIdx.x, K = k + 1;
+    const size_t fo[3] = {(size_t)F_TT * v.uf, (size_t)F_RO * v.uf, (size_t)F_BY * v.uf};
+    const int nf = lmag ? 3 : 2;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const float* uf32 = static_cast<const float*>(v.u);
+    const double* uf64 = static_cast<const double*>(v.u);
+    for (int q = threadIdx.x; q < npx * npy; q += HM_THREADS) {
         const int i = q % npx + 1, j = q / npx + 1;
-        st += uget(v, F_TT, i, j, k + 1);
-        sr += uget(v, F_RO, i, j, k + 1);
-        if (lmag) sb += uget(v, F_BY, i, j, k + 1);
+        const size_t off = (size_t)K * v.uz + (size_t)j * v.upitch + i;
+        for (int t = 0; t < nf; ++t) acc[t] += v.f32 ? (double)uf32[fo[t] + off] : uf64[fo[t] + off];
     }
-    double* outs[3] = {&st, &sr, &sb};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int t = 0; t < 3; ++t) {
-        red[threadIdx.x] = *outs[t];
-        __syncthreads();
-        for (int w = 128; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
+        double x = acc[t];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[t][wid] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int t = 0; t < 3; ++t) {
+            double x = lane < HM_THREADS / 32 ? red[t][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) {
+                // background rows of the FP32 form: RO 0, TT 1, BY 3
+                const double bg = v.f32 ? v.bgd[(t == 0 ? 1 : t == 1 ? 0 : 3) * v.NZ + K] : 0.0;
+                means[t * npz + k] = (t < nf ? bg + x / ((double)npx * npy) : 0.0);
+            }
         }
-        if (threadIdx.x == 0) means[t * npz + k] = red[0] / ((double)npx * npy);
-        __syncthreads();
     }
 }
 
@@ -513,41 +526,70 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 // with the grid's metric factors (HX*DXXDX ...), zero on the wall planes.
 // Output field f (RU,RV,RW,TT,BX,BY,BZ) at out[f*fstride + k*kstride + j*jstride + i].
 // flag[0] is set when an output is not finite or the stress exceeds trip x RO*TT.
-__global__ void k_tendency(UView v, const float* __restrict__ pred, const float* __restrict__ osc,
-                           const double* __restrict__ fax, const double* __restrict__ fay,
-                           const double* __restrict__ faz, int npx, int npy, int npz, float trip,
-                           float* __restrict__ out, size_t fstride, size_t kstride, size_t jstride, int* flag)
+__global__ void __launch_bounds__(256) k_tendency(UView v, const float* __restrict__ pred,
+                                                  const float* __restrict__ osc, const double* __restrict__ fax,
+                                                  const double* __restrict__ fay, const double* __restrict__ faz,
+                                                  int npx, int npy, int npz, float trip, float* __restrict__ out,
+                                                  size_t fstride, size_t kstride, size_t jstride, int* flag)
 {
     const size_t n = (size_t)npx * npy * npz;
+    const size_t sy = (size_t)npx * 16, sz = (size_t)npx * npy * 16;   // pred strides of y and z
+    float s[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) s[c] = osc[c];
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(q % npx), j = (int)((q / npx) % npy), k = (int)(q / ((size_t)npx * npy));
         float* o = out + (size_t)k * kstride + (size_t)j * jstride + i;
         const float* pc = pred + q * 16;
+        // rows are 64-byte aligned: channels 0..11 as three 16-byte loads
+        auto row12 = [](const float* r, float (&v)[12]) {
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
+                const float4 a = __ldg(reinterpret_cast<const float4*>(r) + h);
+                v[4 * h] = a.x;
+                v[4 * h + 1] = a.y;
+                v[4 * h + 2] = a.z;
+                v[4 * h + 3] = a.w;
+            }
+        };
+        float cv[12];
+        row12(pc, cv);
         bool bad = false;
-        for (int c = 0; c < 12; ++c) bad |= !isfinite(pc[c]);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) bad |= !isfinite(cv[c]);
         const double ro = uget(v, F_RO, i + 1, j + 1, k + 1), tt = uget(v, F_TT, i + 1, j + 1, k + 1);
-        const double tr = (fabs((double)pc[0] * osc[0]) + fabs((double)pc[1] * osc[1]) + fabs((double)pc[2] * osc[2]));
+        const double tr = fabs((double)(cv[0] * s[0])) + fabs((double)(cv[1] * s[1])) + fabs((double)(cv[2] * s[2]));
         if (bad || !(tr <= (double)trip * ro * tt)) atomicOr(flag, 1);
         if (k == 0 || k == npz - 1) {
+#pragma unroll
             for (int f = 0; f < 7; ++f) o[f * fstride] = 0.f;
             continue;
         }
-        const int ip = i + 1 == npx ? 0 : i + 1, im = i == 0 ? npx - 1 : i - 1;
-        const int jp = j + 1 == npy ? 0 : j + 1, jm = j == 0 ? npy - 1 : j - 1;
-        auto P = [&](int ii, int jj, int kk, int c) -> double {
-            return (double)pred[(((size_t)kk * npy + jj) * npx + ii) * 16 + c] * osc[c];
-        };
-        const double ax = fax[i + 1], ay = fay[j + 1], az = faz[k + 1];
-        auto dx = [&](int c) { return (P(ip, j, k, c) - P(im, j, k, c)) * ax; };
-        auto dy = [&](int c) { return (P(i, jp, k, c) - P(i, jm, k, c)) * ay; };
-        auto dz = [&](int c) { return (P(i, j, k + 1, c) - P(i, j, k - 1, c)) * az; };
-        o[0 * fstride] = (float)(-(dx(0) + dy(3) + dz(4)));
-        o[1 * fstride] = (float)(-(dx(3) + dy(1) + dz(5)));
-        o[2 * fstride] = (float)(-(dx(4) + dy(5) + dz(2)));
-        o[3 * fstride] = (float)(-(dx(6) + dy(7) + dz(8)) / ro);
-        o[4 * fstride] = (float)(dy(11) - dz(10));
-        o[5 * fstride] = (float)(dz(9) - dx(11));
-        o[6 * fstride] = (float)(dx(10) - dy(9));
+        // neighbours along x and y wrap periodically
+        const float* xp = pc + (i + 1 == npx ? -(ptrdiff_t)(npx - 1) * 16 : 16);
+        const float* xm = pc - (i == 0 ? -(ptrdiff_t)(npx - 1) * 16 : 16);
+        const float* yp = pc + (j + 1 == npy ? -(ptrdiff_t)(npy - 1) * (ptrdiff_t)sy : (ptrdiff_t)sy);
+        const float* ym = pc - (j == 0 ? -(ptrdiff_t)(npy - 1) * (ptrdiff_t)sy : (ptrdiff_t)sy);
+        const float* zp = pc + sz;
+        const float* zm = pc - sz;
+        const float ax = (float)fax[i + 1], ay = (float)fay[j + 1], az = (float)faz[k + 1];
+        float vxp[12], vxm[12], vyp[12], vym[12], vzp[12], vzm[12];
+        row12(xp, vxp);
+        row12(xm, vxm);
+        row12(yp, vyp);
+        row12(ym, vym);
+        row12(zp, vzp);
+        row12(zm, vzm);
+        auto dx = [&](int c) { return (vxp[c] - vxm[c]) * s[c] * ax; };
+        auto dy = [&](int c) { return (vyp[c] - vym[c]) * s[c] * ay; };
+        auto dz = [&](int c) { return (vzp[c] - vzm[c]) * s[c] * az; };
+        o[0 * fstride] = -(dx(0) + dy(3) + dz(4));
+        o[1 * fstride] = -(dx(3) + dy(1) + dz(5));
+        o[2 * fstride] = -(dx(4) + dy(5) + dz(2));
+        o[3 * fstride] = -(dx(6) + dy(7) + dz(8)) / (float)ro;
+        o[4 * fstride] = dy(11) - dz(10);
+        o[5 * fstride] = dz(9) - dx(11);
+        o[6 * fstride] = dx(10) - dy(9);
     }
 }
 
@@ -1431,7 +1473,7 @@ int closure_eval(Handle* h, int cur)
     const size_t nv = (size_t)npx * npy * npz;
     const UView v = uview(h, cur);
     CK(cudaMemsetAsync(h->cflag, 0, sizeof(int), h->st));
-    k_hmeans3<<<npz, 256, 0, h->st>>>(v, npx, npy, h->cmeans, npz, h->p.lmag);
+    k_hmeans3<<<npz, HM_THREADS, 0, h->st>>>(v, npx, npy, h->cmeans, npz, h->p.lmag);
     k_features<<<grid_for(nv), 256, 0, h->st>>>(v, h->cmeans, h->cin_scale, npx, npy, npz, h->p.lmag, h->cfeat);
     CK(cudaGetLastError());
     int32_t* err = h->cflag + 3;
@@ -2002,7 +2044,7 @@ int mhd3d_closure_features(void* handle, const float* in_scale, void* feat, doub
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const UView v = uview(h, h->cur);
-    k_hmeans3<<<npz, 256, 0, s>>>(v, npx, npy, means, npz, h->p.lmag);
+    k_hmeans3<<<npz, HM_THREADS, 0, s>>>(v, npx, npy, means, npz, h->p.lmag);
     k_features<<<grid_for((size_t)npx * npy * npz), 256, 0, s>>>(v, means, in_scale, npx, npy, npz, h->p.lmag,
                                                                 static_cast<__nv_bfloat16*>(feat));
     CK(cudaGetLastError());
@@ -2033,7 +2075,8 @@ int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_sca
                            float trip, void* stream)
 {
     Handle* h = static_cast<Handle*>(handle);
-    if (!h || !pred || !out_scale || !out || !flag) return MHD3D_ERR_ARG;
+    // pred rows are read as 16-byte vectors
+    if (!h || !pred || (reinterpret_cast<uintptr_t>(pred) & 15u) || !out_scale || !out || !flag) return MHD3D_ERR_ARG;
     CK(cudaSetDevice(h->dev));
     if (int st = settle(h)) return st;
     CK(cudaStreamSynchronize(h->st));
