@@ -8,19 +8,17 @@
 // of one (y, z) row, n = output channel, k = tap*CIN + input channel.
 //
 //  - k_conv3d (forward, and the input gradient with transposed, flipped
-//    weights): tcgen05.mma (kind::f16, BF16 in, FP32 accumulator in TMEM,
-//    M=128, N=COUT, K=16 per instruction) issued by one thread.  The input
-//    block of a row (130 x 3 x 3 voxels) sits in shared memory as
-//    [8-channel chunk][voxel] 16-byte rows, which is the canonical K-major
-//    no-swizzle layout with 8-row groups 128 bytes apart: the A operand of
-//    tap (dx,dy,dz) is the same descriptor moved by whole 16-byte rows.  The
-//    weights stay in shared memory in the same canonical layout for all rows
-//    of the persistent CTA.  The accumulator is read back with tcgen05.ld;
-//    the epilogue adds the bias, applies ReLU or the ReLU mask of the layer
-//    below, and writes BF16 (and FP32) outputs.  A CTA walks a contiguous run
-//    of rows along y and keeps a ring of four y rows (each with its z
-//    neighbours): a tile loads one new row, by cp.async, while the previous
-//    tile's MMAs run, and the taps address the ring's slots.
+//    weights): tcgen05.mma (kind::f16, BF16 in, FP32 accumulators in TMEM,
+//    M=128, K=16 per instruction) issued by one thread.  Input rows (130 x
+//    3 z planes) sit in a shared-memory ring as [8-channel chunk][voxel]
+//    16-byte rows, the canonical K-major no-swizzle layout with 8-row groups
+//    128 bytes apart, so the A operand of tap (dx, dz) is one descriptor moved
+//    by whole 16-byte rows.  One MMA serves three output rows (N = 3*COUT,
+//    the y taps stacked in the B operand), see k_conv3d.  Warp roles: a
+//    loader (TMA boxes, or cp.async when nx is not a multiple of 128), one
+//    MMA thread and four epilogue warps, handing off through mbarriers.  The
+//    epilogue adds the bias, applies ReLU or the ReLU mask of the layer
+//    below, and writes BF16 (and FP32) outputs.
 //  - k_conv3d_wgrad: dW[n][tap*CIN+ci] = sum over voxels of dY[v][n] *
 //    X[v+tap][ci], an FP32 CUDA-core reduction (its M = COUT is below the
 //    64 rows of a tcgen05 instruction and its K runs over all voxels).
@@ -259,71 +257,22 @@ __device__ __forceinline__ void tmem_st_zero<32>(uint32_t taddr)
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// The steps of a CTA.  Its range of output rows is split into two halves,
-// each walked as runs along y within one (x segment, z) column; a run of
-// output rows ya..yb takes input rows ya-1..yb+1, one step each.  The steps of
-// the two halves alternate (then the longer half finishes alone), so that two
-// accumulator sets take turns on the tensor cores.  f(s, X, k, x0, z, r,
-// first, emit) for every step s in order: X the half (accumulator set), k the
-// step's index within its half, r the unwrapped input row, first the run's
-// first step, emit whether output row r-1 is in the run; f returns false to
-// stop.
-constexpr bool TWO_SETS = false;   // alternate two halves of the range (measured slower: more runs)
-
-struct RunCursor {
-    int t, t_end, ny, nz, ya, yb, z, x0, r;
-    bool live;
-    __device__ void start_run()
-    {
-        live = t < t_end;
-        if (!live) return;
-        ya = t % ny;
-        z = (t / ny) % nz;
-        x0 = (t / (ny * nz)) * MT;
-        const int run = (t_end - t) < (ny - ya) ? (t_end - t) : (ny - ya);
-        yb = ya + run - 1;
-        r = ya - 1;
-        t += run;
-    }
-    __device__ void next()
-    {
-        if (++r > yb + 1) start_run();
-    }
-};
-
+// The steps of a CTA: its range of output rows forms runs along y within one
+// (x segment, z) column; a run of output rows ya..yb takes input rows
+// ya-1..yb+1, one step each.  f(s, x0, z, r, first, emit) for every step s in
+// order: r the unwrapped input row, first the run's first step, emit whether
+// output row r-1 is in the run; f returns false to stop.
 template <class F>
 __device__ __forceinline__ void for_steps(int t_begin, int t_end, int ny, int nz, F f)
 {
-    const int t_mid = TWO_SETS ? t_begin + (t_end - t_begin) / 2 : t_begin;
-    // a: the half whose turn it is (the second, longer half leads); swapped
-    // rather than indexed so the cursors stay in registers
-    RunCursor a, b;
-    a.t = t_mid;
-    a.t_end = t_end;
-    b.t = t_begin;
-    b.t_end = t_mid;
-    a.ny = b.ny = ny;
-    a.nz = b.nz = nz;
-    a.start_run();
-    b.start_run();
-    int xa = 1, xb = 0, ka = 0, kb = 0;
-    auto swap_ab = [&]() {
-        const RunCursor tc = a;
-        a = b;
-        b = tc;
-        const int tx = xa;
-        xa = xb;
-        xb = tx;
-        const int tk = ka;
-        ka = kb;
-        kb = tk;
-    };
-    for (int s = 0; a.live || b.live; ++s) {
-        if (!a.live) swap_ab();
-        if (!f(s, xa, ka, a.x0, a.z, a.r, a.r == a.ya - 1, a.r - 1 >= a.ya && a.r - 1 <= a.yb)) return;
-        a.next();
-        ++ka;
-        if (b.live) swap_ab();
+    int s = 0;
+    for (int t = t_begin; t < t_end;) {
+        const int ya = t % ny, z = (t / ny) % nz, x0 = (t / (ny * nz)) * MT;
+        const int run = (t_end - t) < (ny - ya) ? (t_end - t) : (ny - ya);
+        const int yb = ya + run - 1;
+        for (int r = ya - 1; r <= yb + 1; ++r, ++s)
+            if (!f(s, x0, z, r, r == ya - 1, r - 1 >= ya && r - 1 <= yb)) return;
+        t += run;
     }
 }
 
@@ -332,15 +281,14 @@ struct ConvLay {
     static constexpr int K = 27 * CIN;
     static constexpr int KB = 9 * CIN;          // K of one y-tap block: (dz, dx, ci)
     static constexpr int NW = 3 * COUT;         // N of an MMA: three output rows
-    static constexpr uint32_t SET = NW <= 64 ? 64 : 128;   // TMEM columns of one accumulator set
-    static constexpr uint32_t NCOL = 2 * SET;
+    static constexpr uint32_t NCOL = NW <= 32 ? 32 : NW <= 64 ? 64 : 128;   // TMEM: three accumulator slots
     static constexpr size_t W_B = (size_t)5 * COUT * KB * 2;   // y-tap blocks 2, 1, 0, 2, 1
     static constexpr size_t X_OFF = (W_B + 127) / 128 * 128;
     static constexpr size_t X_B = ((size_t)CIN * RSEG * 2 + 127) / 128 * 128;  // ring of RING input rows
     static constexpr size_t BAR_OFF = X_OFF + X_B;
-    // barriers: ready[4], mmadone[4], accfull[2], accempty[2]; then the TMEM
+    // barriers: ready[4], mmadone[4], accfull, accempty; then the TMEM
     // address, the abort flag and the last committed step
-    static constexpr size_t BYTES = BAR_OFF + 12 * 8 + 16 + 128;
+    static constexpr size_t BYTES = BAR_OFF + 10 * 8 + 16 + 128;
 };
 
 // Y = act(conv(X, W) + bias) [* (mask > 0)], persistent over (x segment, y, z) tiles.
@@ -359,17 +307,19 @@ struct ConvLay {
 // stores.  The first MMA of a run starts all three slots from zero.
 //
 // Warp roles, pipelined over the CTA's steps s (ready and mmadone by s & 3):
-//   warps 4..4+NLW-1 (loaders): cp.async of the step's input row (three z
-//     planes, periodic in x and y, zeros outside z) into ring slot s % RING;
-//     each thread's copies arrive on ready(s) as they land
-//     (cp.async.mbarrier.arrive), and the slot is reused once the MMAs of
-//     step s - RING have completed (mmadone).
-//   warp 4+NLW, lane 0 (MMA): waits ready(s) and the release of its set's
-//     previous step (accempty), issues the step's MMAs into that set,
-//     commits to the set's accfull and to mmadone(s).  While one set's
-//     finished slot is read out, the MMAs of the other set's step run.
-//   warps 0-3 (epilogue): wait accfull of the step's set, read and zero the
-//     finished slot (TMEM lanes 32*warp..), release it (accempty) and store.
+//   loaders: the step's input row (three z planes, periodic in x and y,
+//     zeros outside z) into ring slot s % RING.  With use_tma (nx a multiple
+//     of 128) warp 4 alone: one TMA box of 8 channels x 128 voxels per chunk
+//     and z plane (complete_tx on ready(s)) and the two x-halo voxels by
+//     cp.async; otherwise warps 4..4+NLW-1 by cp.async.  Each loader thread's
+//     copies arrive on ready(s) as they land (cp.async.mbarrier.arrive), and a
+//     slot is reused once the MMAs of step s - RING have completed (mmadone).
+//   warp 4+NLW, lane 0 (MMA): waits ready(s) and the release of step s-1's
+//     finished slot (accempty), issues the step's MMAs, commits to accfull
+//     and to mmadone(s).
+//   warps 0-3 (epilogue): wait accfull(s), read and zero the finished slot
+//     (TMEM lanes 32*warp..), release it (accempty) and store while the next
+//     step's MMAs run.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtensorMap xmap, int use_tma,
                                                   const __nv_bfloat16* __restrict__ x,
@@ -387,11 +337,11 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
     unsigned long long* const bars = reinterpret_cast<unsigned long long*>(sb + L::BAR_OFF);
     unsigned long long* const ready = bars;
     unsigned long long* const mmadone = bars + 4;
-    unsigned long long* const accfull = bars + 8;    // per accumulator set
-    unsigned long long* const accempty = bars + 10;  // per accumulator set
-    uint32_t* const tslot = reinterpret_cast<uint32_t*>(sb + L::BAR_OFF + 96);
-    volatile int* const abort_flag = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 100);
-    volatile int* const last_commit = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 104);
+    unsigned long long* const accfull = bars + 8;
+    unsigned long long* const accempty = bars + 9;
+    uint32_t* const tslot = reinterpret_cast<uint32_t*>(sb + L::BAR_OFF + 80);
+    volatile int* const abort_flag = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 84);
+    volatile int* const last_commit = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 88);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // weights -> y-tap blocks 2,1,0,2,1 of [COUT][KB], k' = (dz*3 + dx)*CIN + ci, in
@@ -435,10 +385,8 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
             mbar_init(ready + b, use_tma ? 1 + 32 : 32 * NLW);
             mbar_init(mmadone + b, 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(accfull + b, 1);
-            mbar_init(accempty + b, 4);
-        }
+        mbar_init(accfull, 1);
+        mbar_init(accempty, 4);
         *abort_flag = 0;
         *last_commit = -1;
         fence_mbar_init();
@@ -462,7 +410,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
 
     if (use_tma && warp == 4) {
         // one warp: the TMA boxes of the step's row and its two halo voxels
-        for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int x0, int zz, int r, bool, bool) {
+        for_steps(t_begin, t_end, ny, nz, [&](int s, int x0, int zz, int r, bool, bool) {
             if (*abort_flag) return false;
             const int jw = s - RING;   // slot s % RING was last read by step s - RING
             if (jw >= 0 && !mbar_wait_fast(mmadone + (jw & 3), (unsigned)(jw >> 2) & 1u)) {
@@ -480,7 +428,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
         // each loader thread's copies of step s arrive on ready(s) when they
         // land, so the loaders run ahead as far as the ring allows
         const int tix = tid - 128;
-        for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int x0, int zz, int r, bool, bool) {
+        for_steps(t_begin, t_end, ny, nz, [&](int s, int x0, int zz, int r, bool, bool) {
             if (*abort_flag) return false;
             // slot s % RING was last read by step s - RING
             const int jw = s - RING;
@@ -499,10 +447,10 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
             constexpr uint32_t IDESC = idesc_bf16(MT, L::NW);
             const uint64_t da0 = smem_desc(smem_u32(sx), RSEG * 16, 128);
             const uint64_t db0 = smem_desc(smem_u32(sw), 128, (KB / 8) * 128);
-            for_steps(t_begin, t_end, ny, nz, [&](int s, int X, int k, int, int, int r, bool first, bool) {
+            for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int r, bool first, bool) {
                 if (*abort_flag) return false;
                 if (!mbar_wait_fast(ready + (s & 3), (unsigned)(s >> 2) & 1u) ||
-                    (k > 0 && !mbar_wait_fast(accempty + X, (unsigned)(k - 1) & 1u))) {
+                    (s > 0 && !mbar_wait_fast(accempty, (unsigned)(s - 1) & 1u))) {
                     give_up();
                     return false;
                 }
@@ -520,10 +468,10 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
                         for (int kk = 0; kk < CIN / 16; ++kk) {
                             const uint64_t da = da0 + (uint64_t)(as + (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
                             const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
-                            umma_bf16(tmem + (uint32_t)X * L::SET, da, db, IDESC,
+                            umma_bf16(tmem, da, db, IDESC,
                                       (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
                         }
-                umma_commit(accfull + X);
+                umma_commit(accfull);
                 umma_commit(mmadone + (s & 3));
                 *last_commit = s;
                 return true;
@@ -531,22 +479,22 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
         }
         __syncwarp();
     } else if (warp < 4) {   // loader warps without work (TMA rows) take no role
-        for_steps(t_begin, t_end, ny, nz, [&](int, int X, int k, int x0, int zz, int r, bool, bool emit) {
+        for_steps(t_begin, t_end, ny, nz, [&](int s, int x0, int zz, int r, bool, bool emit) {
             if (*abort_flag) return false;
-            if (!mbar_wait_fast(accfull + X, (unsigned)k & 1u)) {
+            if (!mbar_wait_fast(accfull, (unsigned)s & 1u)) {
                 give_up();
                 return false;
             }
             tc_fence_after();
             const int yo = r - 1;   // the output row this step completes
-            const uint32_t col = (uint32_t)X * L::SET + (uint32_t)((((yo % 3) + 3) % 3) * COUT);
+            const uint32_t col = (uint32_t)((((yo % 3) + 3) % 3) * COUT);
             const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + col;
             float acc[COUT];
             if (emit) tmem_ld<COUT>(ta, acc);
             tmem_st_zero<COUT>(ta);
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(accempty + X);
+            if (lane == 0) mbar_arrive(accempty);
             if (!emit) return true;
             const int m = warp * 32 + lane;
             const bool own = x0 + m < nx;   // for nx < 128 the tile repeats the row's period
