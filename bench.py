@@ -45,6 +45,21 @@ WORKLOAD = dict(npx=512, npy=512, npz=256, ra=1e6, ta=1e6, pr=1.0, pm=4.0, contr
 WORKLOAD_NAME = ("FP64-plain fine run of the closure case: 512x512x256 rotating MHD polytrope, "
                  "Ra=1e6 Ta=1e6 Pr=1 Pm=4 contrast 10 beta=1e4 tanh stretch 1.5")
 SAMPLE_NPZ = 32  # CPU baseline slab
+# the other named cases, at their own sizes and physics (--case); they print
+# the same line for the results table and are not the headline workload
+CASES = {
+    "c1": dict(npx=64, npy=64, npz=48, ra=1e5, ta=1e4, pr=1.0, pm=4.0, contrast=10.0, m=1.0, beta=1e4,
+               stretch=1.5, ampt=2e-4, mode="fast",
+               name="c1: 64x64x48 rotating MHD, Ra=1e5 Ta=1e4 contrast 10, FP64 (state fits in L2)"),
+    "c2": dict(npx=256, npy=256, npz=128, ra=1e6, ta=1e6, pr=1.0, pm=4.0, contrast=10.0, m=1.0, beta=1e4,
+               stretch=1.5, ampt=2e-4, mode="fast", name="c2: 256x256x128 rotating MHD, Ra=1e6 Ta=1e6, FP64"),
+    "c5": dict(npx=1024, npy=1024, npz=512, ra=1e7, ta=1e7, pr=1.0, pm=4.0, contrast=30.0, m=1.0, beta=1e4,
+               stretch=2.0, ampt=2e-4, mode="fp32",
+               name="c5: 1024x1024x512 rotating MHD, Ra=1e7 Ta=1e7 contrast 30 stretch 2, FP32 form"),
+    "c5fp64": dict(npx=768, npy=768, npz=384, ra=1e7, ta=1e7, pr=1.0, pm=4.0, contrast=30.0, m=1.0, beta=1e4,
+                   stretch=2.0, ampt=2e-4, mode="fast",
+                   name="c5 FP64 variant: 768x768x384, Ra=1e7 Ta=1e7 contrast 30 stretch 2, FP64 FMA mode"),
+}
 
 
 def env_int(k, d):
@@ -147,12 +162,13 @@ def decomposition(cores, npy, npz):
     return npey, npez
 
 
-def cpu_reference_run(steps: int, warmup: int, npz: int = SAMPLE_NPZ):
-    """Time the reference's own step (translated build) on a 512x512xnpz slab, all cores."""
+def cpu_reference_run(steps: int, warmup: int, npz: int = SAMPLE_NPZ, work: dict | None = None):
+    """Time the reference's own step (translated build) on an npx x npy x npz slab
+    of the workload (the bench workload unless work is given), all cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mhd3d
     import oracle_py
-    w = dict(WORKLOAD, npz=npz)
+    w = dict(work or WORKLOAD, npz=npz)
     cfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
                                   w["m"], w["beta"], w["stretch"], w["ampt"])
     setup = mhd3d.make_setup(cfg)
@@ -402,8 +418,12 @@ def main():
                     help="fast: FP64 with FMA (default); exact: FP64 reference rounding; fp32: FP32 form")
     ap.add_argument("--grid", type=str, default=None, help="override NPXxNPYxNPZ (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end pass (it pins two host copies of the state)")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-npz", type=int, default=SAMPLE_NPZ)
+    ap.add_argument("--case", choices=sorted(CASES), default=None,
+                    help="time another named case at its own size and physics instead of the bench workload")
     ap.add_argument("--workload", choices=["fine", "ensemble", "closure"], default="fine",
                     help="fine: the 512x512x256 step (default); ensemble: the batched FP32 ensemble "
                          "of 48 uneven grids; closure: the FP32+closure coarse 128x128x64 run")
@@ -437,6 +457,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     w = dict(WORKLOAD)
+    wname = WORKLOAD_NAME
+    if args.case:
+        w = {k: v for k, v in CASES[args.case].items() if k not in ("mode", "name")}
+        wname = CASES[args.case]["name"]
+        args.mode = CASES[args.case]["mode"]
     if args.grid:
         w["npx"], w["npy"], w["npz"] = (int(v) for v in args.grid.lower().split("x"))
     cfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
@@ -505,46 +530,53 @@ def main():
             "stage_ms_per_launch": [m / max(n, 1) for m, n in zip(stage_ms, stage_n)]}
 
     # ---- end to end through the C-ABI with pinned host buffers ----------
-    shape = setup.shape
-    nfort = shape[0] * shape[1] * shape[2]
-    pinned_t = [torch.empty(nfort, dtype=torch.float64, pin_memory=True) for _ in range(2 * nf)]
-    hin = {}
-    hout = {}
-    for i, f in enumerate(mhd3d.FIELDS[:nf]):
-        a = pinned_t[i].numpy().reshape(shape, order="F")
-        a[...] = setup.state[f]
-        hin[f] = a
-        hout[f] = pinned_t[nf + i].numpy().reshape(shape, order="F")
-    e2e_steps = args.steps
-    barrier()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    wt0 = time.perf_counter()
-    f0.record(stream)
-    st = sim.lib.mhd3d_upload(sim.h, *[mhd3d._ptr(hin.get(f)) for f in mhd3d.FIELDS])
-    assert st == 0, st
-    for _ in range(e2e_steps):
-        r = sim.step(1)
-    st = sim.lib.mhd3d_download(sim.h, *[mhd3d._ptr(hout.get(f)) for f in mhd3d.FIELDS])
-    assert st == 0, st
-    f1.record(stream)
-    f1.synchronize()
-    wall_e2e = time.perf_counter() - wt0
-    ms_e2e = max(f0.elapsed_time(f1), wall_e2e * 1e3)
-    ms_e2e = max_over_ranks(ms_e2e, dist)
-    state_bytes = nf * nfort * 8
-    e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": state_bytes / e2e_steps,
-           "d2h_bytes_per_step": state_bytes / e2e_steps + 40,
-           "sequence": f"mhd3d_upload (pinned) + {e2e_steps} x mhd3d_step(1) with DT/TIMC/TIMT/UMACH/NIT read back "
-                       f"+ mhd3d_download (pinned)",
-           "ms": ms_e2e}
+    e2e = None
+    if not args.no_e2e:
+        shape = setup.shape
+        nfort = shape[0] * shape[1] * shape[2]
+        pinned_t = [torch.empty(nfort, dtype=torch.float64, pin_memory=True) for _ in range(2 * nf)]
+        hin = {}
+        hout = {}
+        for i, f in enumerate(mhd3d.FIELDS[:nf]):
+            a = pinned_t[i].numpy().reshape(shape, order="F")
+            a[...] = setup.state[f]
+            hin[f] = a
+            hout[f] = pinned_t[nf + i].numpy().reshape(shape, order="F")
+        e2e_steps = args.steps
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        wt0 = time.perf_counter()
+        f0.record(stream)
+        st = sim.lib.mhd3d_upload(sim.h, *[mhd3d._ptr(hin.get(f)) for f in mhd3d.FIELDS])
+        assert st == 0, st
+        for _ in range(e2e_steps):
+            r = sim.step(1)
+        st = sim.lib.mhd3d_download(sim.h, *[mhd3d._ptr(hout.get(f)) for f in mhd3d.FIELDS])
+        assert st == 0, st
+        f1.record(stream)
+        f1.synchronize()
+        wall_e2e = time.perf_counter() - wt0
+        ms_e2e = max(f0.elapsed_time(f1), wall_e2e * 1e3)
+        ms_e2e = max_over_ranks(ms_e2e, dist)
+        state_bytes = nf * nfort * 8
+        e2e = {"value": world * cells * e2e_steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / e2e_steps,
+               "d2h_bytes_per_step": state_bytes / e2e_steps + 40,
+               "sequence": f"mhd3d_upload (pinned) + {e2e_steps} x mhd3d_step(1) with DT/TIMC/TIMT/UMACH/NIT read back "
+                           f"+ mhd3d_download (pinned)",
+               "ms": ms_e2e}
 
     # ---- CPU baseline (rank 0, N=1) --------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_run(args.cpu_steps, 1)
+            if args.case:
+                # the whole grid when it is small (c1), else a slab of the case's physics
+                cpu = cpu_reference_run(args.cpu_steps, 1, npz=min(w["npz"], args.ref_npz) if w["npz"] > 64
+                                        else w["npz"], work=w)
+            else:
+                cpu = cpu_reference_run(args.cpu_steps, 1)
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"[:200]}
 
@@ -553,9 +585,11 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.mode == "fp32" else "f64",
                 "data": "synthetic: rotating MHD polytrope from the host mirror of STATIC/TUBE model 4/RAN2",
-                "config": {"workload": WORKLOAD_NAME, "grid": [w["npx"], w["npy"], w["npz"]],
+                "config": {"workload": wname, "grid": [w["npx"], w["npy"], w["npz"]],
                            "mode": args.mode, "fields": nf,
-                           "l2": f"state {3 * nf * cells * word / 1e9:.1f} GB in HBM >> 126 MB L2, no flush needed",
+                           "l2": (f"state {3 * nf * cells * word / 1e9:.1f} GB in HBM >> 126 MB L2, no flush needed"
+                                  if 3 * nf * cells * word > 126e6 else
+                                  f"state {3 * nf * cells * word / 1e6:.0f} MB fits in L2: a small, launch-bound case"),
                            "parallelism": f"{world} independent replica(s), one per GPU, no collectives",
                            "last_dt": res["dt"], "nit": res["nit"]},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
