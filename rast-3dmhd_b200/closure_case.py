@@ -283,6 +283,37 @@ def a_priori(net, judge, log):
 TERMS = {"stress": range(0, 6), "heat": range(6, 9), "emf": range(9, 12)}
 
 
+def term_gains(terms):
+    """{group: gain} of a terms string: '+'-joined groups, each with an
+    optional '@gain'; a group without one takes the next explicit gain to its
+    right (so "stress+heat@0.5" scales both), 1 if none follows."""
+    toks = terms.split("+")
+    out, pending = {}, []
+    for tok in toks:
+        name, _, g = tok.partition("@")
+        if name not in TERMS:
+            raise ValueError(f"unknown closure term group {name!r}")
+        pending.append(name)
+        if g:
+            out.update({n: float(g) for n in pending})
+            pending = []
+    out.update({n: 1.0 for n in pending})
+    return out
+
+
+def gain_grid(spec):
+    """Candidate terms strings of a grid "stress+heat:0,0.25;emf:0,0.12": the
+    cross product of one gain per ';'-separated set of groups."""
+    sets = []
+    for part in spec.split(";"):
+        groups, _, gains = part.partition(":")
+        sets.append((groups.split("+"), gains.split(",")))
+    cands = [""]
+    for groups, gains in sets:
+        cands = [c + ("+" if c else "") + "+".join(f"{g}@{v}" for g in groups) for c in cands for v in gains]
+    return cands
+
+
 def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
     """A coarse FP32 run from the judge's filtered start over the window; with
     net, the closure is attached with only the named term groups applied,
@@ -290,12 +321,11 @@ def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
     g = mhd3d.GpuSim(judge["coarse_setup"], mode=mhd3d.MODE_FP32)
     g.upload(judge["start"])
     if net is not None:
-        terms, _, gain = terms.partition("@")
+        gains = term_gains(terms)
         keep = net.out_scale
-        sc = net.out_scale.clone() * (float(gain) if gain else 1.0)
+        sc = net.out_scale.clone()
         for name, idx in TERMS.items():
-            if name not in terms.split("+"):
-                sc[list(idx)] = 0.0
+            sc[list(idx)] *= gains.get(name, 0.0)
         net.out_scale = sc
         net.attach(g, trip=args.trip)
         net.out_scale = keep
@@ -407,6 +437,8 @@ def main(argv=None):
     ap.add_argument("--gains", default=None,
                     help="comma-separated closure gains tried on the training run's window; the best is judged")
     ap.add_argument("--gain-terms", default="stress+heat+emf")
+    ap.add_argument("--gain-grid", default=None,
+                    help="per-group gains tried on the training window, e.g. 'stress+heat:0,0.25;emf:0,0.12'")
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the trained network and the judge run's window (.npz)")
     ap.add_argument("--load", default=None, help="skip the fine runs and training: read a --save file")
@@ -432,14 +464,16 @@ def main(argv=None):
         if args.save:
             save_case(args.save, net, judge, tr, apri, val)
     chosen = None
-    if args.gains and val is not None:
-        # the gain is chosen on the training run's own window, never on the judge's
+    cands = gain_grid(args.gain_grid) if args.gain_grid else (
+        [f"{args.gain_terms}@{gv}" for gv in args.gains.split(",")] if args.gains else [])
+    if cands and val is not None:
+        # the gains are chosen on the training run's own window, never on the judge's
         scores = {}
-        for gv in args.gains.split(","):
-            run = coarse_phase(val, net, args, log, f"validate@{gv}", f"{args.gain_terms}@{gv}")
+        for cand in cands:
+            run = coarse_phase(val, net, args, log, f"validate {cand}", cand)
             err = rel_errors(run["profiles"], val["profiles"])
-            scores[gv] = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
-            log(f"gain {gv}: status {run['status']} mean(ke, fconv, me) error {scores[gv]}")
+            scores[cand] = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
+            log(f"gains {cand}: status {run['status']} mean(ke, fconv, me) error {scores[cand]}")
         ok = {k: v for k, v in scores.items() if v is not None}
         plain_val = rel_errors(coarse_phase(val, None, args, log, "validate plain")["profiles"], val["profiles"])
         chosen = min(ok, key=ok.get) if ok else None
@@ -449,7 +483,7 @@ def main(argv=None):
     runs = [("plain", coarse_phase(judge, None, args, log, "plain"))]
     variants = args.variants.split(",") if args.variants else []
     if chosen is not None:
-        variants.append(f"{args.gain_terms}@{chosen}")
+        variants.append(chosen)
     for v in variants:
         runs.append(("closure" if v == "stress+heat+emf" else f"closure[{v}]",
                      coarse_phase(judge, net, args, log, f"closure[{v}]", v)))

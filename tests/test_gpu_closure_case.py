@@ -28,7 +28,7 @@ def test_closure_case_small(mhd3d, tmp_path):
     assert res["window"][1] > res["window"][0]
     assert res["train"]["pairs"] == 4 and res["train"]["residual"]["pairs"] == 4
     assert set(res["a_priori"]) == {"commutator_error_ratio", "residual_error_ratio", "commutator_vs_residual_ratio"}
-    assert res["train"]["gain_chosen"] in ("1", "0.5")
+    assert res["train"]["gain_chosen"] in ("stress+heat+emf@1", "stress+heat+emf@0.5")
     names = [k for k in res if k == "plain" or k.startswith("closure")]
     assert "plain" in names and len(names) >= 3   # plain, the default variant, the chosen gain
     for k in names:
