@@ -526,71 +526,118 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 // with the grid's metric factors (HX*DXXDX ...), zero on the wall planes.
 // Output field f (RU,RV,RW,TT,BX,BY,BZ) at out[f*fstride + k*kstride + j*jstride + i].
 // flag[0] is set when an output is not finite or the stress exceeds trip x RO*TT.
-__global__ void __launch_bounds__(256) k_tendency(UView v, const float* __restrict__ pred,
-                                                  const float* __restrict__ osc, const double* __restrict__ fax,
-                                                  const double* __restrict__ fay, const double* __restrict__ faz,
-                                                  int npx, int npy, int npz, float trip, float* __restrict__ out,
-                                                  size_t fstride, size_t kstride, size_t jstride, int* flag)
+// Closure tendencies marching in z: a CTA owns a TTX x TTY column tile and a
+// chunk of TZC planes, and keeps four planes of the tile with its one-voxel
+// x/y halo (channels 0..11 of the prediction rows) in shared memory, so each
+// prediction row is read from L2 about once instead of once per neighbour.
+// Plane k+2 is fetched into registers while plane k is formed.
+constexpr int TTX = 32, TTY = 8, TZC = 8;
+constexpr int TPX = TTX + 2, TPY = TTY + 2, TPV = TPX * TPY;   // voxels of a plane tile with halo
+constexpr size_t TEND_SMEM = (size_t)4 * TPV * 12 * sizeof(float);
+__global__ void __launch_bounds__(TTX * TTY) k_tendency(UView v, const float* __restrict__ pred,
+                                                       const float* __restrict__ osc, const double* __restrict__ fax,
+                                                       const double* __restrict__ fay, const double* __restrict__ faz,
+                                                       int npx, int npy, int npz, float trip, float* __restrict__ out,
+                                                       size_t fstride, size_t kstride, size_t jstride, int* flag)
 {
-    const size_t n = (size_t)npx * npy * npz;
-    const size_t sy = (size_t)npx * 16, sz = (size_t)npx * npy * 16;   // pred strides of y and z
+    extern __shared__ __align__(16) float tsm[];   // [slot 0..3][TPV][12], plane p in slot p & 3
+    const int tid = threadIdx.x, tx = tid % TTX, ty = tid / TTX;
+    const int x0 = blockIdx.x * TTX, y0 = blockIdx.y * TTY;
+    const int kc0 = blockIdx.z * TZC, kc1 = kc0 + TZC < npz ? kc0 + TZC : npz;
+    const int gi = x0 + tx, gj = y0 + ty;
+    const bool active = gi < npx && gj < npy;
+    constexpr int NL = (TPV * 3 + TTX * TTY - 1) / (TTX * TTY);   // 16-byte loads per thread and plane
+    // plane p (clamped to the grid: the wall planes have no tendency): fetch
+    // into registers, then store into its slot
+    float4 t[NL];
+    auto fetch_plane = [&](int p) {
+        p = p < 0 ? 0 : (p >= npz ? npz - 1 : p);
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int e = tid + u * TTX * TTY;
+            if (e < TPV * 3) {
+                const int vox = e / 3, h = e % 3;
+                int px = x0 - 1 + vox % TPX, py = y0 - 1 + vox / TPX;
+                px %= npx;
+                px = px < 0 ? px + npx : px;
+                py %= npy;
+                py = py < 0 ? py + npy : py;
+                t[u] = __ldg(reinterpret_cast<const float4*>(pred + (((size_t)p * npy + py) * npx + px) * 16) + h);
+            }
+        }
+    };
+    auto store_plane = [&](int p) {
+        const int slot = (p + 4) & 3;
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int e = tid + u * TTX * TTY;
+            if (e < TPV * 3) *reinterpret_cast<float4*>(tsm + ((size_t)slot * TPV + e / 3) * 12 + 4 * (e % 3)) = t[u];
+        }
+    };
     float s[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) s[c] = osc[c];
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % npx), j = (int)((q / npx) % npy), k = (int)(q / ((size_t)npx * npy));
-        float* o = out + (size_t)k * kstride + (size_t)j * jstride + i;
-        const float* pc = pred + q * 16;
-        // rows are 64-byte aligned: channels 0..11 as three 16-byte loads
-        auto row12 = [](const float* r, float (&v)[12]) {
-#pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                const float4 a = __ldg(reinterpret_cast<const float4*>(r) + h);
-                v[4 * h] = a.x;
-                v[4 * h + 1] = a.y;
-                v[4 * h + 2] = a.z;
-                v[4 * h + 3] = a.w;
-            }
-        };
-        float cv[12];
-        row12(pc, cv);
-        bool bad = false;
-#pragma unroll
-        for (int c = 0; c < 12; ++c) bad |= !isfinite(cv[c]);
-        const double ro = uget(v, F_RO, i + 1, j + 1, k + 1), tt = uget(v, F_TT, i + 1, j + 1, k + 1);
-        const double tr = fabs((double)(cv[0] * s[0])) + fabs((double)(cv[1] * s[1])) + fabs((double)(cv[2] * s[2]));
-        if (bad || !(tr <= (double)trip * ro * tt)) atomicOr(flag, 1);
-        if (k == 0 || k == npz - 1) {
-#pragma unroll
-            for (int f = 0; f < 7; ++f) o[f * fstride] = 0.f;
-            continue;
-        }
-        // neighbours along x and y wrap periodically
-        const float* xp = pc + (i + 1 == npx ? -(ptrdiff_t)(npx - 1) * 16 : 16);
-        const float* xm = pc - (i == 0 ? -(ptrdiff_t)(npx - 1) * 16 : 16);
-        const float* yp = pc + (j + 1 == npy ? -(ptrdiff_t)(npy - 1) * (ptrdiff_t)sy : (ptrdiff_t)sy);
-        const float* ym = pc - (j == 0 ? -(ptrdiff_t)(npy - 1) * (ptrdiff_t)sy : (ptrdiff_t)sy);
-        const float* zp = pc + sz;
-        const float* zm = pc - sz;
-        const float ax = (float)fax[i + 1], ay = (float)fay[j + 1], az = (float)faz[k + 1];
-        float vxp[12], vxm[12], vyp[12], vym[12], vzp[12], vzm[12];
-        row12(xp, vxp);
-        row12(xm, vxm);
-        row12(yp, vyp);
-        row12(ym, vym);
-        row12(zp, vzp);
-        row12(zm, vzm);
-        auto dx = [&](int c) { return (vxp[c] - vxm[c]) * s[c] * ax; };
-        auto dy = [&](int c) { return (vyp[c] - vym[c]) * s[c] * ay; };
-        auto dz = [&](int c) { return (vzp[c] - vzm[c]) * s[c] * az; };
-        o[0 * fstride] = -(dx(0) + dy(3) + dz(4));
-        o[1 * fstride] = -(dx(3) + dy(1) + dz(5));
-        o[2 * fstride] = -(dx(4) + dy(5) + dz(2));
-        o[3 * fstride] = -(dx(6) + dy(7) + dz(8)) / (float)ro;
-        o[4 * fstride] = dy(11) - dz(10);
-        o[5 * fstride] = dz(9) - dx(11);
-        o[6 * fstride] = dx(10) - dy(9);
+    const float ax = active ? (float)fax[gi + 1] : 0.f, ay = active ? (float)fay[gj + 1] : 0.f;
+    const int lc = (ty + 1) * TPX + (tx + 1);   // own voxel in a plane tile
+    for (int p = kc0 - 1; p <= kc0 + 1; ++p) {
+        fetch_plane(p);
+        store_plane(p);
     }
+    for (int k = kc0; k < kc1; ++k) {
+        __syncthreads();                     // planes k-1, k, k+1 are in place
+        if (k + 2 <= kc1) fetch_plane(k + 2);  // in flight while plane k is formed
+        if (active) {
+            const float* Pc = tsm + (size_t)(k & 3) * TPV * 12;
+            const float* Pp = tsm + (size_t)((k + 1) & 3) * TPV * 12;
+            const float* Pm = tsm + (size_t)((k + 3) & 3) * TPV * 12;
+            const float* cv = Pc + lc * 12;
+            float* o = out + (size_t)k * kstride + (size_t)gj * jstride + gi;
+            bool bad = false;
+#pragma unroll
+            for (int c = 0; c < 12; ++c) bad |= !isfinite(cv[c]);
+            const double ro = uget(v, F_RO, gi + 1, gj + 1, k + 1), tt = uget(v, F_TT, gi + 1, gj + 1, k + 1);
+            const double tr =
+                fabs((double)(cv[0] * s[0])) + fabs((double)(cv[1] * s[1])) + fabs((double)(cv[2] * s[2]));
+            if (bad || !(tr <= (double)trip * ro * tt)) atomicOr(flag, 1);
+            if (k == 0 || k == npz - 1) {
+#pragma unroll
+                for (int f = 0; f < 7; ++f) o[f * fstride] = 0.f;
+            } else {
+                const float az = (float)faz[k + 1];
+                const float *xp = cv + 12, *xm = cv - 12, *yp = cv + TPX * 12, *ym = cv - TPX * 12;
+                const float *zp = Pp + lc * 12, *zm = Pm + lc * 12;
+                auto dx = [&](int c) { return (xp[c] - xm[c]) * s[c] * ax; };
+                auto dy = [&](int c) { return (yp[c] - ym[c]) * s[c] * ay; };
+                auto dz = [&](int c) { return (zp[c] - zm[c]) * s[c] * az; };
+                o[0 * fstride] = -(dx(0) + dy(3) + dz(4));
+                o[1 * fstride] = -(dx(3) + dy(1) + dz(5));
+                o[2 * fstride] = -(dx(4) + dy(5) + dz(2));
+                o[3 * fstride] = -(dx(6) + dy(7) + dz(8)) / (float)ro;
+                o[4 * fstride] = dy(11) - dz(10);
+                o[5 * fstride] = dz(9) - dx(11);
+                o[6 * fstride] = dx(10) - dy(9);
+            }
+        }
+        if (k + 2 <= kc1) store_plane(k + 2);   // slot of plane k-2, read by no thread since the last barrier
+    }
+}
+
+cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const Metrics& m, int npx, int npy,
+                            int npz, float trip, float* out, size_t fstride, size_t kstride, size_t jstride,
+                            int* flag, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(k_tendency, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)TEND_SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const dim3 grid((unsigned)((npx + TTX - 1) / TTX), (unsigned)((npy + TTY - 1) / TTY),
+                    (unsigned)((npz + TZC - 1) / TZC));
+    k_tendency<<<grid, TTX * TTY, TEND_SMEM, st>>>(v, pred, osc, m.fax, m.fay, m.faz, npx, npy, npz, trip, out,
+                                                  fstride, kstride, jstride, flag);
+    return cudaGetLastError();
 }
 
 // Adjoint of k_tendency's linear map pred -> tendencies: for output g
@@ -1481,8 +1528,8 @@ int closure_eval(Handle* h, int cur)
         mhd3d_conv3d(32, 32, h->cact1, h->cw[1], h->cb[1], nullptr, 1, h->cact2, nullptr, npx, npy, npz, err, h->st) ||
         mhd3d_conv3d(32, 16, h->cact2, h->cw[2], h->cb[2], nullptr, 0, nullptr, h->cpred, npx, npy, npz, err, h->st))
         return MHD3D_ERR_CUDA;
-    k_tendency<<<grid_for(nv), 256, 0, h->st>>>(v, h->cpred, h->cout_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy,
-                                                npz, h->ctrip, h->cfcl, h->zf, h->zz, (size_t)h->zpitch, h->cflag);
+    CK(launch_tendency(v, h->cpred, h->cout_scale, h->m, npx, npy, npz, h->ctrip, h->cfcl, h->zf, h->zz,
+                       (size_t)h->zpitch, h->cflag, h->st));
     k_trip_count<<<1, 1, 0, h->st>>>(h->cflag);
     CK(cudaGetLastError());
     return MHD3D_OK;
@@ -2082,10 +2129,8 @@ int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_sca
     CK(cudaStreamSynchronize(h->st));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nv = (size_t)npx * npy * npz;
-    k_tendency<<<grid_for(nv), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        uview(h, h->cur), pred, out_scale, h->m.fax, h->m.fay, h->m.faz, npx, npy, npz, trip, out, nv,
-        (size_t)npx * npy, (size_t)npx, flag);
-    CK(cudaGetLastError());
+    CK(launch_tendency(uview(h, h->cur), pred, out_scale, h->m, npx, npy, npz, trip, out, nv, (size_t)npx * npy,
+                       (size_t)npx, flag, static_cast<cudaStream_t>(stream)));
     return MHD3D_OK;
 }
 
