@@ -56,6 +56,7 @@ struct Handle {
     __nv_bfloat16 *cfeat = nullptr, *cact1 = nullptr, *cact2 = nullptr;
     float *cpred = nullptr, *cfcl = nullptr;
     double* cmeans = nullptr;                  // 3 x NPZ horizontal means (T, RO, BY)
+    double* hpart = nullptr;                   // 3 x NPZ x HM_SPLIT partial sums of those means
     int* cflag = nullptr;                      // [0] trip flag of the current evaluation, [1] trips, [2] evaluations, [3] kernel error
     float ctrip = 1.f;
     Scalars32 s32{};
@@ -410,25 +411,27 @@ __global__ void k_fort_wrap(double* __restrict__ a, int nf, int npx, int npy, in
     }
 }
 
-// per-plane horizontal means of TT, RO, BY (network features): one CTA per
-// plane; the FP32 form sums the perturbations and adds the plane's background
-// once
-constexpr int HM_THREADS = 1024;
-__global__ void __launch_bounds__(HM_THREADS) k_hmeans3(UView v, int npx, int npy, double* __restrict__ means,
+// per-plane horizontal means of TT, RO, BY (network features), in two passes
+// with a fixed summation order: HM_SPLIT CTAs per plane write partial sums,
+// then one thread per (field, plane) adds them in order; the FP32 form sums
+// the perturbations and adds the plane's background once
+constexpr int HM_THREADS = 256, HM_SPLIT = 8;
+__global__ void __launch_bounds__(HM_THREADS) k_hmeans3(UView v, int npx, int npy, double* __restrict__ part,
                                                         int npz, int lmag)
 {
     __shared__ double red[3][HM_THREADS / 32];
-    const int k = blockIdx.x, K = k + 1;
+    const int k = blockIdx.x, K = k + 1, b = blockIdx.y;
     const size_t fo[3] = {(size_t)F_TT * v.uf, (size_t)F_RO * v.uf, (size_t)F_BY * v.uf};
     const int nf = lmag ? 3 : 2;
     double acc[3] = {0.0, 0.0, 0.0};
     const float* uf32 = static_cast<const float*>(v.u);
     const double* uf64 = static_cast<const double*>(v.u);
-    for (int q = threadIdx.x; q < npx * npy; q += HM_THREADS) {
-        const int i = q % npx + 1, j = q / npx + 1;
-        const size_t off = (size_t)K * v.uz + (size_t)j * v.upitch + i;
-        for (int t = 0; t < nf; ++t) acc[t] += v.f32 ? (double)uf32[fo[t] + off] : uf64[fo[t] + off];
-    }
+    // rows j of this CTA's share, x along the threads
+    for (int j = b; j < npy; j += HM_SPLIT)
+        for (int i = threadIdx.x; i < npx; i += HM_THREADS) {
+            const size_t off = (size_t)K * v.uz + (size_t)(j + 1) * v.upitch + (i + 1);
+            for (int t = 0; t < nf; ++t) acc[t] += v.f32 ? (double)uf32[fo[t] + off] : uf64[fo[t] + off];
+        }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int t = 0; t < 3; ++t) {
         double x = acc[t];
@@ -436,44 +439,70 @@ __global__ void __launch_bounds__(HM_THREADS) k_hmeans3(UView v, int npx, int np
         if (lane == 0) red[t][wid] = x;
     }
     __syncthreads();
-    if (wid == 0) {
-        for (int t = 0; t < 3; ++t) {
-            double x = lane < HM_THREADS / 32 ? red[t][lane] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-            if (lane == 0) {
-                // background rows of the FP32 form: RO 0, TT 1, BY 3
-                const double bg = v.f32 ? v.bgd[(t == 0 ? 1 : t == 1 ? 0 : 3) * v.NZ + K] : 0.0;
-                means[t * npz + k] = (t < nf ? bg + x / ((double)npx * npy) : 0.0);
-            }
-        }
+    if (threadIdx.x < 3) {
+        double x = 0.0;
+        for (int w = 0; w < HM_THREADS / 32; ++w) x += red[threadIdx.x][w];
+        part[((size_t)threadIdx.x * npz + k) * HM_SPLIT + b] = x;
     }
 }
 
+__global__ void k_hmeans3_fin(UView v, const double* __restrict__ part, int npx, int npy, int npz, int lmag,
+                              double* __restrict__ means)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;   // t * npz + k
+    if (q >= 3 * npz) return;
+    const int t = q / npz, k = q % npz;
+    const int nf = lmag ? 3 : 2;
+    double x = 0.0;
+    for (int b = 0; b < HM_SPLIT; ++b) x += part[(size_t)q * HM_SPLIT + b];
+    // background rows of the FP32 form: RO 0, TT 1, BY 3
+    const double bg = v.f32 ? v.bgd[(t == 0 ? 1 : t == 1 ? 0 : 3) * v.NZ + k + 1] : 0.0;
+    means[q] = t < nf ? bg + x / ((double)npx * npy) : 0.0;
+}
+
 // network input, channels-last BF16 [k][j][i][16]: u, v, w, TT-<TT>, RO-<RO>, BX, BY-<BY>, BZ
-// times in_scale, channels 8..15 zero
+// times in_scale, channels 8..15 zero; grid (x blocks, y, z)
 __global__ void k_features(UView v, const double* __restrict__ means, const float* __restrict__ sc, int npx, int npy,
                            int npz, int lmag, __nv_bfloat16* __restrict__ feat)
 {
-    const size_t n = (size_t)npx * npy * npz;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % npx) + 1, j = (int)((q / npx) % npy) + 1, k = (int)(q / ((size_t)npx * npy));
-        const double ro = uget(v, F_RO, i, j, k + 1), ri = 1.0 / ro;
-        float f[8];
-        f[0] = (float)(uget(v, F_RU, i, j, k + 1) * ri);
-        f[1] = (float)(uget(v, F_RV, i, j, k + 1) * ri);
-        f[2] = (float)(uget(v, F_RW, i, j, k + 1) * ri);
-        f[3] = (float)(uget(v, F_TT, i, j, k + 1) - means[k]);
-        f[4] = (float)(ro - means[npz + k]);
-        f[5] = lmag ? (float)uget(v, F_BX, i, j, k + 1) : 0.f;
-        f[6] = lmag ? (float)(uget(v, F_BY, i, j, k + 1) - means[2 * npz + k]) : 0.f;
-        f[7] = lmag ? (float)uget(v, F_BZ, i, j, k + 1) : 0.f;
-        __align__(16) __nv_bfloat16 h[16];
-        for (int c = 0; c < 8; ++c) h[c] = __float2bfloat16_rn(f[c] * sc[c]);
-        for (int c = 8; c < 16; ++c) h[c] = __float2bfloat16_rn(0.f);
-        uint4* o = reinterpret_cast<uint4*>(feat + q * 16);
-        o[0] = reinterpret_cast<const uint4*>(h)[0];
-        o[1] = reinterpret_cast<const uint4*>(h)[1];
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x, j0 = blockIdx.y, k = blockIdx.z;
+    if (i0 >= npx) return;
+    const int i = i0 + 1, j = j0 + 1;
+    const size_t q = ((size_t)k * npy + j0) * npx + i0;
+    const double ro = uget(v, F_RO, i, j, k + 1), ri = 1.0 / ro;
+    float f[8];
+    f[0] = (float)(uget(v, F_RU, i, j, k + 1) * ri);
+    f[1] = (float)(uget(v, F_RV, i, j, k + 1) * ri);
+    f[2] = (float)(uget(v, F_RW, i, j, k + 1) * ri);
+    f[3] = (float)(uget(v, F_TT, i, j, k + 1) - means[k]);
+    f[4] = (float)(ro - means[npz + k]);
+    f[5] = lmag ? (float)uget(v, F_BX, i, j, k + 1) : 0.f;
+    f[6] = lmag ? (float)(uget(v, F_BY, i, j, k + 1) - means[2 * npz + k]) : 0.f;
+    f[7] = lmag ? (float)uget(v, F_BZ, i, j, k + 1) : 0.f;
+    __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) h[c] = __float2bfloat16_rn(f[c] * sc[c]);
+#pragma unroll
+    for (int c = 8; c < 16; ++c) h[c] = __float2bfloat16_rn(0.f);
+    uint4* o = reinterpret_cast<uint4*>(feat + q * 16);
+    o[0] = reinterpret_cast<const uint4*>(h)[0];
+    o[1] = reinterpret_cast<const uint4*>(h)[1];
+}
+
+// features of the handle's current state with the per-plane means (means: 3 x NPZ)
+cudaError_t launch_features(Handle* h, const UView& v, const float* in_scale, double* means, __nv_bfloat16* feat,
+                            cudaStream_t st)
+{
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    if (!h->hpart) {
+        const cudaError_t e = cudaMalloc(&h->hpart, sizeof(double) * 3 * npz * HM_SPLIT);
+        if (e != cudaSuccess) return e;
     }
+    k_hmeans3<<<dim3((unsigned)npz, HM_SPLIT), HM_THREADS, 0, st>>>(v, npx, npy, h->hpart, npz, h->p.lmag);
+    k_hmeans3_fin<<<(unsigned)((3 * npz + 127) / 128), 128, 0, st>>>(v, h->hpart, npx, npy, npz, h->p.lmag, means);
+    k_features<<<dim3((unsigned)((npx + 127) / 128), (unsigned)npy, (unsigned)npz), 128, 0, st>>>(
+        v, means, in_scale, npx, npy, npz, h->p.lmag, feat);
+    return cudaGetLastError();
 }
 
 // mean-square error over 12 channels and its gradient (BF16, channels 12..15 zero)
@@ -916,6 +945,7 @@ int destroy(Handle* h)
     cudaFree(h->z);
     cudaFree(h->stage);
     cudaFree(h->fout);
+    cudaFree(h->hpart);
     cudaFree(h->met);
     cudaFree(h->bgd);
     cudaFree(h->bg32);
@@ -1517,11 +1547,9 @@ UView uview(const Handle* h, int cur)
 int closure_eval(Handle* h, int cur)
 {
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
-    const size_t nv = (size_t)npx * npy * npz;
     const UView v = uview(h, cur);
     CK(cudaMemsetAsync(h->cflag, 0, sizeof(int), h->st));
-    k_hmeans3<<<npz, HM_THREADS, 0, h->st>>>(v, npx, npy, h->cmeans, npz, h->p.lmag);
-    k_features<<<grid_for(nv), 256, 0, h->st>>>(v, h->cmeans, h->cin_scale, npx, npy, npz, h->p.lmag, h->cfeat);
+    CK(launch_features(h, v, h->cin_scale, h->cmeans, h->cfeat, h->st));
     CK(cudaGetLastError());
     int32_t* err = h->cflag + 3;
     if (mhd3d_conv3d(16, 32, h->cfeat, h->cw[0], h->cb[0], nullptr, 1, h->cact1, nullptr, npx, npy, npz, err, h->st) ||
@@ -1573,6 +1601,7 @@ int closure_set(Handle* h, const void* const w[3], const float* const b[3], cons
         h->cmeans = reinterpret_cast<double*>(base + omeans);
         h->cflag = reinterpret_cast<int*>(base + oflag);
     }
+    if (!h->hpart) CK(cudaMalloc(&h->hpart, sizeof(double) * 3 * h->p.npz * HM_SPLIT));   // not in the step path
     for (int l = 0; l < 3; ++l) {
         CK(cudaMemcpyAsync(h->cw[l], w[l], wn[l] * 2, cudaMemcpyDefault, h->st));
         CK(cudaMemcpyAsync(h->cb[l], b[l], bn[l] * 4, cudaMemcpyDefault, h->st));
@@ -2089,12 +2118,8 @@ int mhd3d_closure_features(void* handle, const float* in_scale, void* feat, doub
     if (int st = settle(h)) return st;
     CK(cudaStreamSynchronize(h->st));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const UView v = uview(h, h->cur);
-    k_hmeans3<<<npz, HM_THREADS, 0, s>>>(v, npx, npy, means, npz, h->p.lmag);
-    k_features<<<grid_for((size_t)npx * npy * npz), 256, 0, s>>>(v, means, in_scale, npx, npy, npz, h->p.lmag,
-                                                                static_cast<__nv_bfloat16*>(feat));
-    CK(cudaGetLastError());
+    CK(launch_features(h, v, in_scale, means, static_cast<__nv_bfloat16*>(feat), s));
     return MHD3D_OK;
 }
 
