@@ -11,6 +11,10 @@
 //              with its halo is one in-bounds TMA box.  Field-major, x fastest.
 //   Z        : nf fields x NPZ x NPY x zpitch, interior cells only.
 #pragma once
+
+#ifndef MHD3D_MINB
+#define MHD3D_MINB 3   // FP64 stage CTAs per SM: 3 x 128 threads x 168 registers, 3 x 65 KB shared
+#endif
 #include <cuda.h>
 #include <cuda_runtime.h>
 

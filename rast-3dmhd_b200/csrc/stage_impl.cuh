@@ -35,7 +35,13 @@ namespace MHD3D_NS {
 
 enum Q { Q_RU = 0, Q_RV, Q_RW, Q_RO, Q_TT, Q_RI, Q_UU, Q_VV, Q_WW, Q_P, Q_BX, Q_BY, Q_BZ };
 
-constexpr int NRAW = 4;   // raw-plane ring slots (planes k-1, k, k+1 in use, k+2 in flight)
+#ifndef MHD3D_NRAW
+#define MHD3D_NRAW 4
+#endif
+// raw-plane ring slots: planes k-1, k, k+1 in use and, with 4, plane k+2 in
+// flight (with 3 the next plane is issued when plane k-1's slot frees)
+constexpr int NRAW = MHD3D_NRAW;
+static_assert(NRAW == 3 || NRAW == 4, "three or four ring slots");
 constexpr int NRI = 3;    // 1/RO ring slots (planes k-1, k, k+1)
 
 template <bool MAG>
@@ -215,22 +221,22 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     // it is the ((kp-(k0-1))>>2)-th fill of its slot
     int hi_issued = k0 - 2;   // thread 0: highest plane issued so far
     auto issue_plane = [&](int kp) {
-        const int sl = (kp + 1) & 3;
+        const int sl = (kp + 1) % NRAW;
         fence_proxy_async();
         mbar_expect_tx(&bars[sl], raw_bytes);
         tma_load4(sraw + (size_t)sl * L::RAW_SLOT, &a.map_u, &bars[sl], x0, y0, kp + 1, 0);
         hi_issued = kp;
     };
-    auto parity_of = [&](int kp) -> unsigned { return (unsigned)(((kp - (k0 - 1)) >> 2) & 1); };
+    auto parity_of = [&](int kp) -> unsigned { return (unsigned)(((kp - (k0 - 1)) / NRAW) & 1); };
     auto derive_ri = [&](int kp) {
-        const double* r = sraw + (size_t)((kp + 1) & 3) * L::RAW_SLOT + F_RO * BSLOT;
+        const double* r = sraw + (size_t)((kp + 1) % NRAW) * L::RAW_SLOT + F_RO * BSLOT;
         double* d = sri + (size_t)((kp + 1) % 3) * BSLOT;
         for (int p = tid; p < BSLOT; p += NT) d[p] = 1.0 / r[p];
     };
 
     if (tid == 0)
-        for (int kp = k0 - 1; kp <= k0 + 2 && kp <= k1; ++kp) issue_plane(kp);
-    bool ok = mbar_wait(&bars[(k0 + 0) & 3], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) & 3], parity_of(k0));
+        for (int kp = k0 - 1; kp <= k0 - 2 + NRAW && kp <= k1; ++kp) issue_plane(kp);
+    bool ok = mbar_wait(&bars[(k0 + 0) % NRAW], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) % NRAW], parity_of(k0));
     if (ok) {
         derive_ri(k0 - 1);
         derive_ri(k0);
@@ -248,15 +254,15 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
             tma_load4(sz, &a.map_z, &bars[NRAW], x0, y0, k, 0);
             zpending = true;
         }
-        if (!mbar_wait(&bars[(k + 2) & 3], parity_of(k + 1))) atomicOr(sflag, 1);
+        if (!mbar_wait(&bars[(k + 2) % NRAW], parity_of(k + 1))) atomicOr(sflag, 1);
         else derive_ri(k + 1);
         __syncthreads();
         if (*sflag) break;
         bool zok = true;
         if (active) {
-            const double* Rm = sraw + (size_t)((k + 0) & 3) * L::RAW_SLOT;   // plane k-1
-            const double* Rc = sraw + (size_t)((k + 1) & 3) * L::RAW_SLOT;   // plane k
-            const double* Rp = sraw + (size_t)((k + 2) & 3) * L::RAW_SLOT;   // plane k+1
+            const double* Rm = sraw + (size_t)((k + 0) % NRAW) * L::RAW_SLOT;   // plane k-1
+            const double* Rc = sraw + (size_t)((k + 1) % NRAW) * L::RAW_SLOT;   // plane k
+            const double* Rp = sraw + (size_t)((k + 2) % NRAW) * L::RAW_SLOT;   // plane k+1
             const double* Im = sri + (size_t)((k + 0) % 3) * BSLOT;
             const double* Ic = sri + (size_t)((k + 1) % 3) * BSLOT;
             const double* Ip = sri + (size_t)((k + 2) % 3) * BSLOT;
@@ -762,16 +768,16 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         }
         __syncthreads();
         if (*sflag) break;
-        // refill: plane k+3 goes to the slot plane k-1 has left
-        if (tid == 0 && k + 3 <= k1) issue_plane(k + 3);
+        // refill: plane k+NRAW-1 goes to the slot plane k-1 has left
+        if (tid == 0 && k + NRAW - 1 <= k1) issue_plane(k + NRAW - 1);
     }
     if (*sflag) {
         // a bounded wait gave up: let every fill still in flight land (again
         // bounded), report, and leave without touching the reduction
         if (tid == 0) {
-            // the last fill of each slot is one of the four highest planes issued
-            for (int kp = hi_issued - 3; kp <= hi_issued; ++kp)
-                if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) & 3], parity_of(kp));
+            // the last fill of each slot is one of the NRAW highest planes issued
+            for (int kp = hi_issued - (NRAW - 1); kp <= hi_issued; ++kp)
+                if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) % NRAW], parity_of(kp));
             if (zpending) mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
             atomicExch(&a.ctl->status, MHD3D_ERR_TIMEOUT);
             atomicExch(&a.ctl->stop, 1);
