@@ -1,7 +1,6 @@
 """Unit tests of the Fortran-subset translator (oracle/fortran_subset.py)."""
 import os
 import subprocess
-import tempfile
 
 import pytest
 
