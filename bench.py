@@ -386,6 +386,81 @@ def run_closure(args, rank, world, local):
     dt_coarse = res["dt"]
     fine_cells = w["npx"] * w["npy"] * w["npz"]
     fine_equiv = fine_cells * (dt_coarse / dt_fine) * args.steps / (ms / 1e3) / 1e6
+
+    # tensor roofline of the convolutions: the three layers of one evaluation,
+    # timed alone (CUDA events on the launching stream), against the burst
+    # BF16 peak; algorithmic FLOPs 2*27*(8*32 + 32*32 + 32*12) per voxel (the
+    # 8 real input channels and 12 real outputs)
+    lib = mhd3d.gpu_lib()
+    nz, ny, nx = 64, 128, 128
+    nvox = nx * ny * nz
+    P = lambda t: mhd3d.C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    with torch.cuda.stream(stream):
+        feat = (torch.randn((nz, ny, nx, 16), device="cuda") * 0.5).to(torch.bfloat16)
+        a1 = torch.empty((nz, ny, nx, 32), dtype=torch.bfloat16, device="cuda")
+        a2 = torch.empty_like(a1)
+        pred = torch.empty((nz, ny, nx, 16), dtype=torch.float32, device="cuda")
+    cerr = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sh = mhd3d.C.c_void_p(stream.cuda_stream)
+
+    def evaluation():
+        for cin, cout, src, dst, dstf, li, relu in ((16, 32, feat, a1, None, 0, 1), (32, 32, a1, a2, None, 1, 1),
+                                                    (32, 16, a2, None, pred, 2, 0)):
+            st = lib.mhd3d_conv3d(cin, cout, P(src), P(net.w16[li]), P(net.b[li]), None, relu, P(dst), P(dstf),
+                                  nx, ny, nz, P(cerr), sh)
+            assert st == 0, st
+    for _ in range(3):
+        evaluation()
+    reps = 20
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    c0.record(stream)
+    for _ in range(reps):
+        evaluation()
+    c1.record(stream)
+    c1.synchronize()
+    conv_ms = c0.elapsed_time(c1) / reps
+    alg_flop = 2.0 * 27 * (8 * 32 + 32 * 32 + 32 * 12) * nvox
+    peaks, peak_kind = measured_peaks()
+    peak_tf = peaks.get("bf16_tflops", 1590.0)
+    achieved_tf = alg_flop / (conv_ms / 1e3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": achieved_tf / peak_tf, "traffic": None,
+            "kernel": "k_conv3d (three layers of one closure evaluation, timed alone)",
+            "algorithmic_flop_per_evaluation": alg_flop, "ms_per_evaluation": conv_ms,
+            "peak_source": "measured MEASURED_PEAKS.json bf16_tflops (burst)" if peak_kind == "measured"
+            else "fallback 1.59 PFLOP/s"}
+
+    # end to end through the C-ABI: upload from pinned memory, K steps with
+    # the closure, download
+    shape = setup.shape
+    nfort = shape[0] * shape[1] * shape[2]
+    nf = 8 if cfg.lmag else 5
+    pin = [torch.empty(nfort, dtype=torch.float64, pin_memory=True) for _ in range(2 * nf)]
+    hin, hout = {}, {}
+    for i, f in enumerate(mhd3d.FIELDS[:nf]):
+        a = pin[i].numpy().reshape(shape, order="F")
+        a[...] = setup.state[f]
+        hin[f] = a
+        hout[f] = pin[nf + i].numpy().reshape(shape, order="F")
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    wt0 = time.perf_counter()
+    f0.record(stream)
+    assert sim.lib.mhd3d_upload(sim.h, *[mhd3d._ptr(hin.get(f)) for f in mhd3d.FIELDS]) == 0
+    for _ in range(args.steps):
+        sim.step(1)
+    assert sim.lib.mhd3d_download(sim.h, *[mhd3d._ptr(hout.get(f)) for f in mhd3d.FIELDS]) == 0
+    f1.record(stream)
+    f1.synchronize()
+    ms_e2e = max(f0.elapsed_time(f1), (time.perf_counter() - wt0) * 1e3)
+    state_bytes = nf * nfort * 8
+    e2e = {"value": world * cells * args.steps / (ms_e2e / 1e3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps + 40,
+           "sequence": f"mhd3d_upload (pinned) + {args.steps} x mhd3d_step(1) with the closure + mhd3d_download",
+           "ms": ms_e2e}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -397,11 +472,12 @@ def run_closure(args, rank, world, local):
                            "closure": {"evals": status["evals"], "trips": status["trips"], "err": status["err"]},
                            "dt_coarse": dt_coarse, "dt_fine_first_step": dt_fine,
                            "fine_equivalent_mcell_steps_per_s": fine_equiv,
-                           "fine_equivalent_note": "512^2*256 cells x (DT_coarse/DT_fine) per coarse step; assumes "
-                                                   "the closure holds the fine run's flux error (not demonstrated)",
+                           "fine_equivalent_note": "512^2*256 cells x (DT_coarse/DT_fine) per coarse step; the "
+                                                   "profile criterion is shown at half size only "
+                                                   "(profiles/closure_case_256x256x128.md)",
                            "parallelism": f"{world} independent replica(s), one per GPU, no collectives"},
-                "roofline": None, "cpu_baseline": None,
-                "e2e": None, "gpu_launches": 10 * args.steps, "clocks": clk}
+                "roofline": roof, "cpu_baseline": None,
+                "e2e": e2e, "gpu_launches": 12 * args.steps, "clocks": clk}
         print(json.dumps(line), flush=True)
     sim.close()
     return 0
