@@ -195,6 +195,33 @@ def cpu_reference_run(steps: int, warmup: int, npz: int = SAMPLE_NPZ, work: dict
                       f"RK3 steps, {how}; {secs:.2f} s"}
 
 
+def cpu_compare(steps: int, npz: int = SAMPLE_NPZ):
+    """The CPU baselines side by side on the bench workload's slab: the C
+    restatement (oracle, OpenMP) at 1 thread and at all host cores, and the
+    translated reference STEP with its MPI decomposition; one JSON line."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mhd3d
+    import oracle_py
+    w = dict(WORKLOAD, npz=npz)
+    cfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
+                                  w["m"], w["beta"], w["stretch"], w["ampt"])
+    setup = mhd3d.make_setup(cfg)
+    cells = w["npx"] * w["npy"] * w["npz"]
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    out = {"cpu_compare": True, "unit": UNIT, "slab": [w["npx"], w["npy"], w["npz"]], "steps": steps,
+           "host_cores": cores}
+    for threads in (1, cores):
+        oracle_py.set_threads(threads)
+        o = oracle_py.Oracle(setup.params, setup.grid, setup.state)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(steps)
+        out[f"oracle_{threads}_threads"] = cells * steps / (time.perf_counter() - t0) / 1e6
+    if oracle_py.reference_available():
+        out["reference_mpi"] = cpu_reference_run(steps, 1, npz=npz)
+    print(json.dumps(out), flush=True)
+
+
 def run_reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -493,6 +520,8 @@ def main():
                     help="fast: FP64 with FMA (default); exact: FP64 reference rounding; fp32: FP32 form")
     ap.add_argument("--grid", type=str, default=None, help="override NPXxNPYxNPZ (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-compare", action="store_true",
+                    help="only time the CPU baselines (oracle at 1 and all threads, translated reference)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end pass (it pins two host copies of the state)")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -510,6 +539,9 @@ def main():
     rank = env_int("RANK", 0)
     local = env_int("LOCAL_RANK", 0)
 
+    if args.cpu_compare:
+        cpu_compare(args.cpu_steps, args.ref_npz)
+        return 0
     if args.impl == "reference":
         line = run_reference_arm(args, rank, world)
         if line is not None:
