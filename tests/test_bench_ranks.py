@@ -44,3 +44,28 @@ def test_single_rank_passthrough():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks(3.5, None) == 3.5
+
+
+def test_reference_decomposition():
+    """The emulated MPI layout of the CPU reference: NPEY*NPEZ ranks, a power
+    of two within the cores, NPEZ dividing NPZ with at least 4 planes each."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for cores, npy, npz in ((16, 512, 32), (8, 512, 32), (12, 64, 48), (1, 64, 48), (64, 512, 32)):
+        npey, npez = bench.decomposition(cores, npy, npz)
+        p = npey * npez
+        assert p <= cores and p & (p - 1) == 0
+        assert npz % npez == 0 and npz // npez >= 4
+        assert npy % npey == 0
+
+
+def test_named_cases_match_their_configs():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert [bench.CASES["c1"][k] for k in ("npx", "npy", "npz", "ra", "ta")] == [64, 64, 48, 1e5, 1e4]
+    assert [bench.CASES["c2"][k] for k in ("npx", "npy", "npz", "ra", "ta")] == [256, 256, 128, 1e6, 1e6]
+    c5, c5d = bench.CASES["c5"], bench.CASES["c5fp64"]
+    assert (c5["npx"], c5["npy"], c5["npz"], c5["mode"]) == (1024, 1024, 512, "fp32")
+    assert (c5d["npx"], c5d["npy"], c5d["npz"], c5d["mode"]) == (768, 768, 384, "fast")
+    for c in (c5, c5d):
+        assert (c["ra"], c["ta"], c["contrast"], c["stretch"]) == (1e7, 1e7, 30.0, 2.0)
