@@ -10,10 +10,12 @@
 //  - k_conv3d (forward, and the input gradient with transposed, flipped
 //    weights): tcgen05.mma (kind::f16, BF16 in, FP32 accumulators in TMEM,
 //    M=128, K=16 per instruction) issued by one thread.  Input rows (130 x
-//    3 z planes) sit in a shared-memory ring as [8-channel chunk][voxel]
-//    16-byte rows, the canonical K-major no-swizzle layout with 8-row groups
-//    128 bytes apart, so the A operand of tap (dx, dz) is one descriptor moved
-//    by whole 16-byte rows.  One MMA serves three output rows (N = 3*COUT,
+//    3 z planes) sit in a shared-memory ring, so the A operand of tap
+//    (dx, dz) is one descriptor moved by whole voxel rows: with 32 input
+//    channels and x a multiple of 128, 64-byte voxel rows in the copy
+//    engine's 64-byte swizzle (one TMA box per plane); otherwise
+//    [8-channel chunk][voxel] 16-byte rows, the canonical K-major no-swizzle
+//    layout with 8-row groups 128 bytes apart.  One MMA serves three output rows (N = 3*COUT,
 //    the y taps stacked in the B operand), see k_conv3d.  Warp roles: a
 //    loader (TMA boxes, or cp.async when nx is not a multiple of 128), one
 //    MMA thread and four epilogue warps, handing off through mbarriers.  The
@@ -142,9 +144,10 @@ __device__ __forceinline__ void load_block_async(unsigned char* sx, const __nv_b
     }
 }
 // Ring of input rows for the convolution: [chunk][slot 0..RING-1][z plane 0..2]
-// [BXP] of 16-byte rows, voxel xi (x0-1+xi) at row XR0+xi, so that the 128
-// interior voxels start on a 128-byte boundary (a TMA destination); step s of
-// a CTA keeps its input row in slot s % RING.
+// [BXP] of 16-byte rows (or, in the swizzled form, [slot][z plane][BXP] of
+// 64-byte rows), voxel xi (x0-1+xi) at row XR0+xi, so that the 128 interior
+// voxels start on a 128-byte (512-byte) boundary, a TMA destination; step s
+// of a CTA keeps its input row in slot s % RING.
 constexpr int XR0 = 7;
 constexpr int BXP = 144;              // XR0 + BX rounded up to 8 rows
 constexpr int RSEG = RING * 3 * BXP;  // voxel rows of one chunk of the ring
@@ -216,6 +219,66 @@ __device__ __forceinline__ void load_row_tma(unsigned char* ring, const CUtensor
     }
 }
 
+// The input row of a step by TMA for 32 input channels, in the 64-byte
+// swizzled K-major layout: plane p = slot*3 + zi of the ring is BXP voxel
+// rows of 64 bytes (all 32 channels) from byte p*BXP*64, and the 16-byte
+// chunk j (channels 8j..8j+7) of row R sits at chunk position j ^ ((R >> 1) & 3)
+// -- the copy engine's SWIZZLE_64B pattern (address bits 4-5 XOR bits 7-8,
+// planes 512-byte aligned), which SWIZZLE_64B matrix descriptors read back.
+// One 4-D box (32 channels, 128 x, 1 y, 1 z) per plane lands the interior at
+// row XR0+1; the two periodic halo voxels come by cp.async, placed by the
+// same rule.
+__device__ __forceinline__ void load_row_tma_sw64(unsigned char* ring, const CUtensorMap* map,
+                                                  unsigned long long* bar, const __nv_bfloat16* __restrict__ x,
+                                                  int x0, int yr, int z, int nx, int ny, int nz, int lane, int slot)
+{
+    constexpr int CIN = 32;
+    int gy = yr % ny;
+    gy = gy < 0 ? gy + ny : gy;
+    const uint32_t sbase = smem_u32(ring);
+    if (lane == 0) {
+        for (int zi = 0; zi < 3; ++zi) {
+            const uint32_t dst = sbase + (uint32_t)(((slot * 3 + zi) * BXP + XR0 + 1) * 64);
+            asm volatile(
+                "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                "%3, %4, %5}], [%6];" ::"r"(dst),
+                "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(x0), "r"(gy), "r"(z - 1 + zi),
+                "r"(smem_u32(bar))
+                : "memory");
+        }
+    }
+    if (lane < 24) {
+        const int side = lane & 1, j = (lane >> 1) & 3, zi = lane >> 3;
+        const int xi = side ? BX - 1 : 0;
+        int gx = x0 - 1 + xi;
+        gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+        int gz = z - 1 + zi;
+        const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
+        gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
+        const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + j * 8;
+        const int R = XR0 + xi;
+        const uint32_t dst = sbase + (uint32_t)(((slot * 3 + zi) * BXP + R) * 64 + ((j ^ ((R >> 1) & 3)) * 16));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(nbytes) : "memory");
+    }
+}
+
+// shared-memory matrix descriptor of a K-major operand in the 64-byte swizzled
+// layout: 64-byte rows, 8-row groups 512 bytes apart (the leading offset is
+// unused when the K of one MMA lies inside a row), SM100 version 1, base
+// offset 0.  The pattern follows the absolute address bits, so a start moved
+// by whole rows (an x tap) or by 32 bytes inside a row (the second K half)
+// reads the rows the copy engine wrote there (checked against the numpy
+// convolution by the GPU parity tests).
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr)
+{
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(512 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
+
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -283,12 +346,12 @@ struct ConvLay {
     static constexpr int NW = 3 * COUT;         // N of an MMA: three output rows
     static constexpr uint32_t NCOL = NW <= 32 ? 32 : NW <= 64 ? 64 : 128;   // TMEM: three accumulator slots
     static constexpr size_t W_B = (size_t)5 * COUT * KB * 2;   // y-tap blocks 2, 1, 0, 2, 1
-    static constexpr size_t X_OFF = (W_B + 127) / 128 * 128;
+    static constexpr size_t X_OFF = (W_B + 1023) / 1024 * 1024;   // the ring's planes 512-byte aligned
     static constexpr size_t X_B = ((size_t)CIN * RSEG * 2 + 127) / 128 * 128;  // ring of RING input rows
     static constexpr size_t BAR_OFF = X_OFF + X_B;
     // barriers: ready[4], mmadone[4], accfull, accempty; then the TMEM
     // address, the abort flag and the last committed step
-    static constexpr size_t BYTES = BAR_OFF + 10 * 8 + 16 + 128;
+    static constexpr size_t BYTES = BAR_OFF + 10 * 8 + 16 + 1024;   // + alignment of the base to 1024 bytes
 };
 
 // Y = act(conv(X, W) + bias) [* (mask > 0)], persistent over (x segment, y, z) tiles.
@@ -309,9 +372,11 @@ struct ConvLay {
 // Warp roles, pipelined over the CTA's steps s (ready and mmadone by s & 3):
 //   loaders: the step's input row (three z planes, periodic in x and y,
 //     zeros outside z) into ring slot s % RING.  With use_tma (nx a multiple
-//     of 128) warp 4 alone: one TMA box of 8 channels x 128 voxels per chunk
-//     and z plane (complete_tx on ready(s)) and the two x-halo voxels by
-//     cp.async; otherwise warps 4..4+NLW-1 by cp.async.  Each loader thread's
+//     of 128) warp 4 alone: one TMA box per z plane of 32 channels x 128
+//     voxels in 64-byte swizzled rows (CIN = 32), or of 8 channels x 128
+//     voxels per chunk and plane (CIN = 16), complete_tx on ready(s), and
+//     the two x-halo voxels by cp.async; otherwise warps 4..4+NLW-1 by
+//     cp.async.  Each loader thread's
 //     copies arrive on ready(s) as they land (cp.async.mbarrier.arrive), and a
 //     slot is reused once the MMAs of step s - RING have completed (mmadone).
 //   warp 4+NLW, lane 0 (MMA): waits ready(s) and the release of step s-1's
@@ -331,7 +396,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
     using L = ConvLay<CIN, COUT>;
     constexpr int K = L::K, KB = L::KB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    unsigned char* const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     unsigned char* const sw = sb;
     unsigned char* const sx = sb + L::X_OFF;
     unsigned long long* const bars = reinterpret_cast<unsigned long long*>(sb + L::BAR_OFF);
@@ -419,7 +484,8 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
             }
             unsigned long long* const bar = ready + (s & 3);
             if (lane == 0) mbar_expect_tx(bar, (unsigned)(CIN / 8 * 3 * MT * 16));
-            load_row_tma<CIN>(sx, &xmap, bar, x, x0, r, zz, nx, ny, nz, lane, s % RING);
+            if constexpr (CIN == 32) load_row_tma_sw64(sx, &xmap, bar, x, x0, r, zz, nx, ny, nz, lane, s % RING);
+            else load_row_tma<CIN>(sx, &xmap, bar, x, x0, r, zz, nx, ny, nz, lane, s % RING);
             asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
             return true;
         });
@@ -446,6 +512,7 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
         if (lane == 0) {
             constexpr uint32_t IDESC = idesc_bf16(MT, L::NW);
             const uint64_t da0 = smem_desc(smem_u32(sx), RSEG * 16, 128);
+            const uint64_t da0s = smem_desc_sw64(smem_u32(sx));
             const uint64_t db0 = smem_desc(smem_u32(sw), 128, (KB / 8) * 128);
             for_steps(t_begin, t_end, ny, nz, [&](int s, int, int, int r, bool first, bool) {
                 if (*abort_flag) return false;
@@ -460,17 +527,33 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
                 const uint32_t st = (uint32_t)(((1 - r) % 3 + 3) % 3);
                 const uint64_t dbs = db0 + (uint64_t)(st * (COUT / 8) * (KB / 8) * 8);
                 const uint32_t as = (uint32_t)((s % RING) * 3 * BXP + XR0);
+                if (CIN == 32 && use_tma) {
+                    // 64-byte swizzled rows: tap (dz, dx) moves the start by whole
+                    // 64-byte rows, the second K half by 32 bytes inside the row
 #pragma unroll
-                for (int dz = 0; dz < 3; ++dz)
+                    for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-                    for (int dx = 0; dx < 3; ++dx)
+                        for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-                        for (int kk = 0; kk < CIN / 16; ++kk) {
-                            const uint64_t da = da0 + (uint64_t)(as + (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
-                            const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
-                            umma_bf16(tmem, da, db, IDESC,
-                                      (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
-                        }
+                            for (int kk = 0; kk < CIN / 16; ++kk) {
+                                const uint64_t da = da0s + (uint64_t)((as + (uint32_t)(dz * BXP + dx)) * 4 + 2 * kk);
+                                const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
+                                umma_bf16(tmem, da, db, IDESC,
+                                          (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
+                            }
+                } else {
+#pragma unroll
+                    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                        for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                            for (int kk = 0; kk < CIN / 16; ++kk) {
+                                const uint64_t da = da0 + (uint64_t)(as + (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
+                                const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
+                                umma_bf16(tmem, da, db, IDESC,
+                                          (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
+                            }
+                }
                 umma_commit(accfull);
                 umma_commit(mmadone + (s & 3));
                 *last_commit = s;
@@ -610,9 +693,9 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// 5-D tiled TMA map of a BF16 array, no swizzle, zeros outside
-cudaError_t encode_bf16_5d(CUtensorMap* map, void* base, const cuuint64_t dims[5], const cuuint64_t strides[4],
-                           const cuuint32_t box[5])
+// tiled TMA map of a BF16 array of the given rank, zeros outside
+cudaError_t encode_bf16(CUtensorMap* map, int rank, void* base, const cuuint64_t* dims, const cuuint64_t* strides,
+                        const cuuint32_t* box, CUtensorMapSwizzle swz)
 {
     static EncodeTiledFn enc = nullptr;
     if (!enc) {
@@ -623,9 +706,9 @@ cudaError_t encode_bf16_5d(CUtensorMap* map, void* base, const cuuint64_t dims[5
         enc = reinterpret_cast<EncodeTiledFn>(fn);
     }
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, base, dims, strides, box, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
@@ -650,12 +733,21 @@ cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
     const int use_tma = nx % MT == 0 ? 1 : 0;
-    if (use_tma) {
+    if (use_tma && CIN == 32) {
+        // (channel, x, y, z) boxes of 32 channels x 128 voxels, 64-byte swizzled rows
+        const cuuint64_t dims[4] = {(cuuint64_t)CIN, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        const cuuint64_t strides[3] = {(cuuint64_t)CIN * 2, (cuuint64_t)nx * CIN * 2, (cuuint64_t)nx * ny * CIN * 2};
+        const cuuint32_t box[4] = {(cuuint32_t)CIN, (cuuint32_t)MT, 1, 1};
+        if (encode_bf16(&map, 4, const_cast<void*>(x), dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B) != cudaSuccess)
+            return cudaErrorInvalidValue;
+    } else if (use_tma) {
+        // (8 channels, chunk, x, y, z) boxes, 16-byte rows
         const cuuint64_t dims[5] = {8, (cuuint64_t)CIN / 8, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
         const cuuint64_t strides[4] = {16, (cuuint64_t)CIN * 2, (cuuint64_t)nx * CIN * 2,
                                        (cuuint64_t)nx * ny * CIN * 2};
         const cuuint32_t box[5] = {8, 1, (cuuint32_t)MT, 1, 1};
-        if (encode_bf16_5d(&map, const_cast<void*>(x), dims, strides, box) != cudaSuccess) return cudaErrorInvalidValue;
+        if (encode_bf16(&map, 5, const_cast<void*>(x), dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE) != cudaSuccess)
+            return cudaErrorInvalidValue;
     }
     k_conv3d<CIN, COUT><<<grid, CT, L::BYTES, st>>>(
         map, use_tma, static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
