@@ -525,35 +525,30 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
                 tc_fence_after();
                 // window of y-tap blocks for slots 0, 1, 2: starts at (1 - r) mod 3
                 const uint32_t st = (uint32_t)(((1 - r) % 3 + 3) % 3);
-                const uint64_t dbs = db0 + (uint64_t)(st * (COUT / 8) * (KB / 8) * 8);
                 const uint32_t as = (uint32_t)((s % RING) * 3 * BXP + XR0);
-                if (CIN == 32 && use_tma) {
-                    // 64-byte swizzled rows: tap (dz, dx) moves the start by whole
-                    // 64-byte rows, the second K half by 32 bytes inside the row
+                // the step's descriptors first (their low words: the start
+                // addresses; the high words are fixed), then its MMAs back to
+                // back.  Tap (dz, dx) moves the A start by whole voxel rows:
+                // 64-byte rows in the swizzled form (the second K half 32
+                // bytes into the row), 16-byte rows otherwise (the second K
+                // half one chunk of the ring further)
+                constexpr int NM = 9 * CIN / 16, KH = CIN / 16;
+                const bool swz = CIN == 32 && use_tma;
+                const uint64_t dab = swz ? da0s : da0;
+                const uint32_t a0 = (uint32_t)dab + (swz ? as * 4 : as);
+                const uint32_t b0 = (uint32_t)db0 + st * (COUT / 8) * (KB / 8) * 8;
+                uint32_t alo[NM], blo[NM];
 #pragma unroll
-                    for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-                        for (int dx = 0; dx < 3; ++dx)
-#pragma unroll
-                            for (int kk = 0; kk < CIN / 16; ++kk) {
-                                const uint64_t da = da0s + (uint64_t)((as + (uint32_t)(dz * BXP + dx)) * 4 + 2 * kk);
-                                const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
-                                umma_bf16(tmem, da, db, IDESC,
-                                          (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
-                            }
-                } else {
-#pragma unroll
-                    for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-                        for (int dx = 0; dx < 3; ++dx)
-#pragma unroll
-                            for (int kk = 0; kk < CIN / 16; ++kk) {
-                                const uint64_t da = da0 + (uint64_t)(as + (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
-                                const uint64_t db = dbs + (uint64_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
-                                umma_bf16(tmem, da, db, IDESC,
-                                          (first && dz == 0 && dx == 0 && kk == 0) ? 0u : 1u);
-                            }
+                for (int j = 0; j < NM; ++j) {
+                    const int dz = j / (3 * KH), dx = (j / KH) % 3, kk = j % KH;
+                    alo[j] = a0 + (swz ? (uint32_t)((dz * BXP + dx) * 4 + 2 * kk)
+                                       : (uint32_t)(2 * kk * RSEG + dz * BXP + dx));
+                    blo[j] = b0 + (uint32_t)((((dz * 3 + dx) * CIN + kk * 16) >> 3) * 8);
                 }
+                const uint64_t ahi = dab & 0xFFFFFFFF00000000ull, bhi = db0 & 0xFFFFFFFF00000000ull;
+#pragma unroll
+                for (int j = 0; j < NM; ++j)
+                    umma_bf16(tmem, ahi | alo[j], bhi | blo[j], IDESC, (first && j == 0) ? 0u : 1u);
                 umma_commit(accfull);
                 umma_commit(mmadone + (s & 3));
                 *last_commit = s;
