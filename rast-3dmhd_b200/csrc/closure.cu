@@ -36,6 +36,7 @@
 
 #include "../../include/mhd3d.h"
 #include "ring.cuh"
+#include "smem_attr.cuh"
 
 namespace mhd3d {
 namespace clo {
@@ -712,13 +713,9 @@ cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const
                           float* yf, int nx, int ny, int nz, int* err, cudaStream_t st)
 {
     using L = ConvLay<CIN, COUT>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv3d<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)L::BYTES);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t ae = smem_attr_once(attr, reinterpret_cast<const void*>(k_conv3d<CIN, COUT>), L::BYTES);
+    if (ae != cudaSuccess) return ae;
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -754,13 +751,9 @@ template <int CIN, int COUT>
 cudaError_t launch_wgrad_t(const void* x, const void* dy, float* dw, float* db, int nx, int ny, int nz, cudaStream_t st)
 {
     const size_t smem = (size_t)CIN * VB * 2 + (size_t)MT * COUT * 4;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv3d_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t ae = smem_attr_once(attr, reinterpret_cast<const void*>(k_conv3d_wgrad<CIN, COUT>), smem);
+    if (ae != cudaSuccess) return ae;
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -14,6 +14,7 @@
 
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
+#include "smem_attr.cuh"
 
 namespace mhd3d {
 namespace {
@@ -655,13 +656,9 @@ cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const 
                             int npz, float trip, float* out, size_t fstride, size_t kstride, size_t jstride,
                             int* flag, cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(k_tendency, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)TEND_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    const cudaError_t ae = smem_attr_once(attr, reinterpret_cast<const void*>(k_tendency), TEND_SMEM);
+    if (ae != cudaSuccess) return ae;
     const dim3 grid((unsigned)((npx + TTX - 1) / TTX), (unsigned)((npy + TTY - 1) / TTY),
                     (unsigned)((npz + TZC - 1) / TZC));
     k_tendency<<<grid, TTX * TTY, TEND_SMEM, st>>>(v, pred, osc, m.fax, m.fay, m.faz, npx, npy, npz, trip, out,

@@ -24,6 +24,7 @@
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
 #include "ring.cuh"
+#include "smem_attr.cuh"
 
 #define MHD3D_NS f32
 #define MHD3D_FAST_BODY 1
@@ -711,13 +712,9 @@ static cudaError_t launch_stage_t(int stage, const StageArgs32& a, cudaStream_t 
     switch (stage) {
 #define L_(S)                                                                                              \
     case S: {                                                                                              \
-        static bool attr_set = false;                                                                      \
-        if (!attr_set) {                                                                                   \
-            cudaError_t e = cudaFuncSetAttribute(k_stage32<MAG, ROT, S>,                                   \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-            if (e != cudaSuccess) return e;                                                                \
-            attr_set = true;                                                                               \
-        }                                                                                                  \
+        static std::atomic<unsigned long long> attr_set{0};                                                \
+        cudaError_t ae = smem_attr_once(attr_set, reinterpret_cast<const void*>(k_stage32<MAG, ROT, S>), smem); \
+        if (ae != cudaSuccess) return ae;                                                                  \
         k_stage32<MAG, ROT, S><<<grid, NT32, smem, st>>>(a);                                              \
         break;                                                                                             \
     }
@@ -745,13 +742,10 @@ static cudaError_t launch_multi_t(int stage, const StageArgs32* args, const int*
     switch (stage) {
 #define L_(S)                                                                                              \
     case S: {                                                                                              \
-        static bool attr_set = false;                                                                      \
-        if (!attr_set) {                                                                                   \
-            cudaError_t e = cudaFuncSetAttribute(k_stage32_multi<MAG, ROT, S>,                             \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-            if (e != cudaSuccess) return e;                                                                \
-            attr_set = true;                                                                               \
-        }                                                                                                  \
+        static std::atomic<unsigned long long> attr_set{0};                                                \
+        cudaError_t ae = smem_attr_once(attr_set, reinterpret_cast<const void*>(k_stage32_multi<MAG, ROT, S>), \
+                                        smem);                                                             \
+        if (ae != cudaSuccess) return ae;                                                                  \
         if (nblocks > 0)                                                                                   \
             k_stage32_multi<MAG, ROT, S><<<nblocks, NT32, smem, st>>>(args, order, item_base, nmem, counter); \
         break;                                                                                             \

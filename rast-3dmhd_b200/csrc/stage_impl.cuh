@@ -27,6 +27,7 @@
 
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
+#include "smem_attr.cuh"
 #include "cfl_cell.cuh"
 #include "ring.cuh"
 
@@ -876,13 +877,9 @@ static cudaError_t launch_stage_t(int stage, const StageArgs& a, cudaStream_t st
     switch (stage) {
 #define L_(S)                                                                                              \
     case S: {                                                                                              \
-        static bool attr_set = false;                                                                      \
-        if (!attr_set) {                                                                                   \
-            cudaError_t e = cudaFuncSetAttribute(k_stage<MAG, ROT, S>,                                     \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-            if (e != cudaSuccess) return e;                                                                \
-            attr_set = true;                                                                               \
-        }                                                                                                  \
+        static std::atomic<unsigned long long> attr_set{0};                                                \
+        cudaError_t ae = smem_attr_once(attr_set, reinterpret_cast<const void*>(k_stage<MAG, ROT, S>), smem); \
+        if (ae != cudaSuccess) return ae;                                                                  \
         k_stage<MAG, ROT, S><<<grid, NT, smem, st>>>(a);                                                  \
         break;                                                                                             \
     }
