@@ -1,6 +1,6 @@
 """The learned-closure case a posteriori: fine FP64 runs, box-filtered training
 pairs, a network trained on the GPU, and coarse FP32 runs with and without the
-closure judged against the filtered fine run's mean profiles.
+closure scored against the filtered fine run's mean profiles.
 
 Pipeline (every arithmetic step in libmhd3d_gpu.so; torch holds device memory):
 
@@ -10,7 +10,7 @@ Pipeline (every arithmetic step in libmhd3d_gpu.so; torch holds device memory):
    and the 12 subgrid terms (stress, heat flux, EMF).
 2. The three-layer convolutional closure is trained on those pairs by the
    library's forward, backward and Adam kernels.
-3. A second fine run of another seed (the judge) is spun up the same way; its
+3. A second fine run of another seed (the held-out run) is spun up the same way; its
    filtered state at the start of the window starts two coarse FP32 runs,
    one plain and one with the closure attached, over the same window.  The
    filtered fine run's horizontal-mean profiles, averaged over the window's
@@ -28,7 +28,7 @@ truncation error included, not only the subgrid terms).
 
 Prints one JSON object: per-profile relative L2 errors of the time-averaged
 profiles (plain coarse and closure coarse against filtered fine), the closure's
-trip count, the a-priori tendency error on the judge run's last pair, step
+trip count, the a-priori tendency error on the held-out run's last pair, step
 counts, DT and wall times.  A coarse run that stops (non-finite values or DT
 collapse) reports its status and the simulated time it reached.
 
@@ -169,7 +169,7 @@ def fine_phase(args, seed, collect, log):
         if args.resid_steps and (collect or s == args.samples):
             R, ca, r = residual_target(pc, fine, args.resid_steps)
             resid.append((R, ca))
-            if collect:   # the judge's last target lies past its window
+            if collect:   # the held-out run's last target lies past its window
                 wsteps += args.resid_steps
                 wwall += r["wall"]
         log(f"fine{seed} sample {s} t={r['timt']:.4f} dt={r['dt']:.3e} umach={r['umach']:.3e}")
@@ -245,32 +245,32 @@ def train_residual(net, data, resid, pc, args, log):
             "seconds": time.perf_counter() - t0, "weights": w.cpu().tolist()}, w
 
 
-def a_priori(net, judge, log):
-    """Tendency error ratio |pred - true|^2 / |true|^2 on the judge run's
+def a_priori(net, heldout, log):
+    """Tendency error ratio |pred - true|^2 / |true|^2 on the held-out run's
     last pair, whose filtered state is resident in the collector's coarse
     handle (no closure gives 1)."""
     torch = _torch()
-    pc = judge["pc"]
+    pc = heldout["pc"]
     s = torch.cuda.current_stream().cuda_stream
     pad = torch.cat([net.in_scale, torch.ones(8, device="cuda")])
     ones12 = torch.ones(12, device="cuda")
-    f, t = judge["pairs"][-1]
-    if judge["resid"]:
-        pc.load(judge["resid"][-1][1])   # the pair's own filtered state
+    f, t = heldout["pairs"][-1]
+    if heldout["resid"]:
+        pc.load(heldout["resid"][-1][1])   # the pair's own filtered state
     _, p = net.forward((f.float()[..., :16] * pad).to(torch.bfloat16), pc.shape, s)
     true_t, _ = closure.tendencies(pc.coarse, closure.pad_targets(t, ones12), ones12)
     pred_t, _ = closure.tendencies(pc.coarse, p, net.out_scale)
     ratio = ((pred_t - true_t) ** 2).sum().item() / (true_t ** 2).sum().item()
     log(f"a priori tendency error ratio {ratio:.4f}")
     out = {"commutator_error_ratio": ratio}
-    if judge["resid"]:
+    if heldout["resid"]:
         # against the coarse scheme's residual at the same state (weighted as in training)
-        R, ca = judge["resid"][-1]
+        R, ca = heldout["resid"][-1]
         pc.load(ca)
         _, p = net.forward((f.float()[..., :16] * pad).to(torch.bfloat16), pc.shape, s)
         pred_t, _ = closure.tendencies(pc.coarse, p, net.out_scale)
         true_t, _ = closure.tendencies(pc.coarse, closure.pad_targets(t, ones12), ones12)
-        w = judge.get("resid_w")
+        w = heldout.get("resid_w")
         wv = (w if w is not None else torch.ones(7, device="cuda")).view(7, 1, 1, 1)
         den = (wv * R ** 2).sum().item()
         out["residual_error_ratio"] = (wv * (pred_t - R) ** 2).sum().item() / den
@@ -314,12 +314,12 @@ def gain_grid(spec):
     return cands
 
 
-def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
-    """A coarse FP32 run from the judge's filtered start over the window; with
+def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf"):
+    """A coarse FP32 run from the held-out run's filtered start over the window; with
     net, the closure is attached with only the named term groups applied,
     scaled by the gain after '@' (terms "stress+heat@0.5")."""
-    g = mhd3d.GpuSim(judge["coarse_setup"], mode=mhd3d.MODE_FP32)
-    g.upload(judge["start"])
+    g = mhd3d.GpuSim(heldout["coarse_setup"], mode=mhd3d.MODE_FP32)
+    g.upload(heldout["start"])
     if net is not None:
         gains = term_gains(terms)
         keep = net.out_scale
@@ -332,7 +332,7 @@ def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
     profs = [g.profiles()]
     steps, wall, dts = 1, 0.0, []
     status, t_end = 0, 0.0
-    span = judge["t1"] - judge["t0"]
+    span = heldout["t1"] - heldout["t0"]
     t0 = time.perf_counter()
     r = g.step(1, check=False)
     wall += time.perf_counter() - t0
@@ -361,10 +361,10 @@ def coarse_phase(judge, net, args, log, tag, terms="stress+heat+emf"):
 WINDOW_KEYS = ("t0", "t1", "steps", "wall", "spin_steps", "dt_mean", "umach_max")
 
 
-def save_case(path, net, judge, tr, apri, val=None):
-    """The trained network and what the coarse runs are judged on (and, with
+def save_case(path, net, heldout, tr, apri, val=None):
+    """The trained network and what the coarse runs are scored on (and, with
     val, the training run's window for choosing a gain)."""
-    d = {f"start_{f}": a for f, a in judge["start"].items() if a is not None}
+    d = {f"start_{f}": a for f, a in heldout["start"].items() if a is not None}
     if val is not None:
         d.update({f"val_start_{f}": a for f, a in val["start"].items() if a is not None})
         d["val_profiles"] = val["profiles"]
@@ -374,8 +374,8 @@ def save_case(path, net, judge, tr, apri, val=None):
         d[f"b{li}"] = net.b[li].cpu().numpy()
     d["in_scale"] = net.in_scale.cpu().numpy()
     d["out_scale"] = net.out_scale.cpu().numpy()
-    d["profiles"] = judge["profiles"]
-    d["meta"] = np.array(json.dumps({k: judge[k] for k in WINDOW_KEYS} | {"train": tr, "a_priori": apri}))
+    d["profiles"] = heldout["profiles"]
+    d["meta"] = np.array(json.dumps({k: heldout[k] for k in WINDOW_KEYS} | {"train": tr, "a_priori": apri}))
     np.savez(path, **d)
 
 
@@ -391,10 +391,10 @@ def load_case(path, args):
     net.in_scale = torch.tensor(z["in_scale"], device="cuda")
     net.out_scale = torch.tensor(z["out_scale"], device="cuda")
     fnx, fny, fnz = args.fine
-    cs = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args, args.judge_seed))
+    cs = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args, args.heldout_seed))
     start = {f: (z[f"start_{f}"] if f"start_{f}" in z else None) for f in mhd3d.FIELDS}
-    judge = {k: meta[k] for k in WINDOW_KEYS}
-    judge.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
+    heldout = {k: meta[k] for k in WINDOW_KEYS}
+    heldout.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
     val = None
     if "val_profiles" in z:
         val = json.loads(str(z["val_meta"]))
@@ -402,7 +402,7 @@ def load_case(path, args):
         val["profiles"] = z["val_profiles"]
         val["coarse_setup"] = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args,
                                                       args.train_seed))
-    return net, judge, meta["train"], meta["a_priori"], val
+    return net, heldout, meta["train"], meta["a_priori"], val
 
 
 def rel_errors(got, ref):
@@ -430,17 +430,17 @@ def main(argv=None):
     ap.add_argument("--resid-iters", type=int, default=3000)
     ap.add_argument("--resid-lr", type=float, default=1e-3)
     ap.add_argument("--train-seed", type=int, default=101)
-    ap.add_argument("--judge-seed", type=int, default=202)
+    ap.add_argument("--heldout-seed", type=int, default=202)
     ap.add_argument("--net-seed", type=int, default=7)
     ap.add_argument("--variants", default="stress+heat+emf",
                     help="comma-separated closure runs, each a '+'-joined set of stress, heat, emf")
     ap.add_argument("--gains", default=None,
-                    help="comma-separated closure gains tried on the training run's window; the best is judged")
+                    help="comma-separated closure gains tried on the training run's window; the best is scored on the held-out run")
     ap.add_argument("--gain-terms", default="stress+heat+emf")
     ap.add_argument("--gain-grid", default=None,
                     help="per-group gains tried on the training window, e.g. 'stress+heat:0,0.25;emf:0,0.12'")
     ap.add_argument("--out", default=None)
-    ap.add_argument("--save", default=None, help="write the trained network and the judge run's window (.npz)")
+    ap.add_argument("--save", default=None, help="write the trained network and the held-out run's window (.npz)")
     ap.add_argument("--load", default=None, help="skip the fine runs and training: read a --save file")
     args = ap.parse_args(argv)
 
@@ -449,7 +449,7 @@ def main(argv=None):
 
     val = None
     if args.load:
-        net, judge, tr, apri, val = load_case(args.load, args)
+        net, heldout, tr, apri, val = load_case(args.load, args)
     else:
         trainer = fine_phase(args, args.train_seed, True, log)
         net, tr, data = train(trainer["pairs"], args, log)
@@ -458,16 +458,16 @@ def main(argv=None):
         if args.resid_steps:
             tr["residual"], w = train_residual(net, data, trainer["resid"], trainer["pc"], args, log)
         del trainer, data
-        judge = fine_phase(args, args.judge_seed, False, log)
-        judge["resid_w"] = w
-        apri = a_priori(net, judge, log)
+        heldout = fine_phase(args, args.heldout_seed, False, log)
+        heldout["resid_w"] = w
+        apri = a_priori(net, heldout, log)
         if args.save:
-            save_case(args.save, net, judge, tr, apri, val)
+            save_case(args.save, net, heldout, tr, apri, val)
     chosen = None
     cands = gain_grid(args.gain_grid) if args.gain_grid else (
         [f"{args.gain_terms}@{gv}" for gv in args.gains.split(",")] if args.gains else [])
     if cands and val is not None:
-        # the gains are chosen on the training run's own window, never on the judge's
+        # the gains are chosen on the training run's own window, never on the held-out run's
         scores = {}
         for cand in cands:
             run = coarse_phase(val, net, args, log, f"validate {cand}", cand)
@@ -480,19 +480,19 @@ def main(argv=None):
         tr["gain_scores"] = scores
         tr["gain_plain_score"] = float(np.mean([plain_val[n] for n in ("ke", "fconv", "me")]))
         tr["gain_chosen"] = chosen
-    runs = [("plain", coarse_phase(judge, None, args, log, "plain"))]
+    runs = [("plain", coarse_phase(heldout, None, args, log, "plain"))]
     variants = args.variants.split(",") if args.variants else []
     if chosen is not None:
         variants.append(chosen)
     for v in variants:
         runs.append(("closure" if v == "stress+heat+emf" else f"closure[{v}]",
-                     coarse_phase(judge, net, args, log, f"closure[{v}]", v)))
-    ref = judge["profiles"]
+                     coarse_phase(heldout, net, args, log, f"closure[{v}]", v)))
+    ref = heldout["profiles"]
     res = {
         "fine": list(args.fine), "fac": args.fac, "ra": args.ra, "ta": args.ta, "contrast": args.contrast,
-        "window": [judge["t0"], judge["t1"]],
-        "fine_window": {"steps": judge["steps"], "wall_s": judge["wall"], "dt_mean": judge["dt_mean"],
-                        "spin_steps": judge["spin_steps"], "umach_max": judge["umach_max"]},
+        "window": [heldout["t0"], heldout["t1"]],
+        "fine_window": {"steps": heldout["steps"], "wall_s": heldout["wall"], "dt_mean": heldout["dt_mean"],
+                        "spin_steps": heldout["spin_steps"], "umach_max": heldout["umach_max"]},
         "train": tr, "a_priori": apri,
     }
     for name, run in runs:
@@ -501,7 +501,7 @@ def main(argv=None):
         d["profile_rel_bias"] = {n: float((run["profiles"][i] - ref[i]).sum() / max(abs(ref[i].sum()), 1e-300))
                                  for i, n in enumerate(mhd3d.PROFILES)}
         if run["wall_s"] > 0 and run["status"] == 0:
-            d["wall_ratio_fine_over_coarse"] = judge["wall"] / run["wall_s"]
+            d["wall_ratio_fine_over_coarse"] = heldout["wall"] / run["wall_s"]
         res[name] = d
     line = json.dumps(res)
     print(line)

@@ -1,6 +1,6 @@
 """The a posteriori closure case end to end at a tiny size: two fine FP64 runs,
 commutator training and residual fine-tuning, the gain chosen on the training
-run's window, coarse runs judged against the filtered fine profiles, and the
+run's window, coarse runs scored against the filtered fine profiles, and the
 saved case reloaded (the plain coarse run must come out the same)."""
 import math
 import os
