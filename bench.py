@@ -499,9 +499,7 @@ def run_closure(args, rank, world, local):
                            "closure": {"evals": status["evals"], "trips": status["trips"], "err": status["err"]},
                            "dt_coarse": dt_coarse, "dt_fine_first_step": dt_fine,
                            "fine_equivalent_mcell_steps_per_s": fine_equiv,
-                           "fine_equivalent_note": "512^2*256 cells x (DT_coarse/DT_fine) per coarse step; the "
-                                                   "profile criterion is shown at half size only "
-                                                   "(profiles/closure_case_256x256x128.md)",
+                           "fine_equivalent_note": "512^2*256 cells x (DT_coarse/DT_fine) per coarse step",
                            "parallelism": f"{world} independent replica(s), one per GPU, no collectives"},
                 "roofline": roof, "cpu_baseline": None,
                 "e2e": e2e, "gpu_launches": 12 * args.steps, "clocks": clk}

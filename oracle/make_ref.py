@@ -8,7 +8,11 @@ writes is committed (oracle/_ref/ is git-ignored); the binary travels with
 the working tree so the benchmark host can time the reference without the
 reference checkout.
 
-    python oracle/make_ref.py [--src /root/reference]
+    python oracle/make_ref.py [--src DIR] [--if-present]
+
+The checkout's location comes from --src, else the environment variable
+MHD3D_REFERENCE_SRC, else the container's read-only mount.  With
+--if-present a missing checkout is not an error (the GPU box has none).
 """
 from __future__ import annotations
 
@@ -21,10 +25,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from fortran_subset import Translator  # noqa: E402
 
+DEFAULT_SRC = os.environ.get("MHD3D_REFERENCE_SRC", "/root/reference")
+
 UNITS = ["STEP", "FLUXES", "BCON", "COMMUNICATE", "COMM_MPI", "HORIZONTAL_MEAN"]
 
 
-def build(src: str = "/root/reference", out_dir: str | None = None, cc: str = "gcc") -> str:
+def build(src: str = DEFAULT_SRC, out_dir: str | None = None, cc: str = "gcc") -> str:
     out_dir = out_dir or os.path.join(HERE, "_ref")
     sub = os.path.join(src, "3dmhdsub.f")
     par = os.path.join(src, "3dmhdparam.f")
@@ -45,7 +51,11 @@ def build(src: str = "/root/reference", out_dir: str | None = None, cc: str = "g
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=DEFAULT_SRC)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--if-present", action="store_true",
+                    help="exit quietly when the reference checkout is absent")
     a = ap.parse_args()
+    if a.if_present and not os.path.isdir(a.src):
+        sys.exit(0)
     print(build(a.src, a.out))

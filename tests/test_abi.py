@@ -56,18 +56,3 @@ def test_bad_arguments_rejected_before_device_use(mhd3d):
     for nx in (0, 96, 200):
         assert lib.mhd3d_conv3d(16, 32, p, p, None, None, 0, p, None, nx, 4, 4, err, None) == 1
         assert lib.mhd3d_conv3d_wgrad(16, 32, p, p, C.cast(buf, C.POINTER(C.c_float)), None, nx, 4, 4, None) == 1
-
-
-def test_integration_table_lists_every_entry_point():
-    """INTEGRATION.md's table names each declared function (families written
-    as `prefix` / `_suffix` count through their suffixes)."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    table = text[text.index("## Entry points at a glance"):]
-    named = set(re.findall(r"`(mhd3d_\w+)`", table))
-    for row in re.findall(r"^\| `(mhd3d_\w+)`(.*?)\|", table, re.M):
-        head, rest = row
-        stem = head.rsplit("_", 1)[0]
-        named |= {stem + s for s in re.findall(r"`(_\w+)`", rest)}
-    for header in ("mhd3d.h", "mhd3d_host.h"):
-        for n in _declared(header):
-            assert n in named, n
