@@ -29,22 +29,36 @@ constexpr int NKEY = 6;   // w1..w4 minima, Mach^2 maximum, non-finite flag
 // Per-plane partial results; sized for MHD3D_NOALLOC_MAX_PLANES planes.
 static __device__ __align__(256) unsigned long long g_cfl_partials[MHD3D_NOALLOC_MAX_PLANES * NKEY];
 
-// Host-side address of g_cfl_partials on each device, looked up once per
-// device with that device current (the symbol's host name is not a device
-// address).
+// Device address of g_cfl_partials in the current device's context.  The
+// symbol's host-side name is not a device address, so it is looked up with
+// the device current.  The lookup runs again on every call made outside a
+// stream capture: after cudaDeviceReset (or any teardown of the primary
+// context) the module is loaded again, possibly at another address, and a
+// remembered address would be stale.  A call whose stream is being captured
+// reuses the address the last uncaptured call on this device found, so the
+// first call on a device has to come before any capture.
 constexpr int MAX_DEVICES = 64;
 static void* g_partials_addr[MAX_DEVICES];
 static std::mutex g_mutex;
 
-static int partials_address(int dev, void** out)
+static int partials_address(int dev, cudaStream_t st, void** out)
 {
     if (dev < 0 || dev >= MAX_DEVICES) return MHD3D_ERR_ARG;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    bool capturing = false;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        (void)cudaGetLastError();   // the query's own error is not the caller's
+        capturing = true;
+    } else {
+        capturing = cap != cudaStreamCaptureStatusNone;
+    }
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_partials_addr[dev]) {
+    if (!capturing) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_cfl_partials) != cudaSuccess || !p) return MHD3D_ERR_CUDA;
         g_partials_addr[dev] = p;
     }
+    if (!g_partials_addr[dev]) return MHD3D_ERR_CUDA;
     *out = g_partials_addr[dev];
     return MHD3D_OK;
 }
@@ -155,8 +169,9 @@ extern "C" int mhd3d_cfl_noalloc(const mhd3d_params* p,
     if (p->npz > MHD3D_NOALLOC_MAX_PLANES) return MHD3D_ERR_ARG;   // the scratch holds one row per plane
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MHD3D_ERR_NO_DEVICE;
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
     void* partials = nullptr;
-    int st = noalloc::partials_address(dev, &partials);
+    int st = noalloc::partials_address(dev, cs, &partials);
     if (st) return st;
     Scalars s{};
     s.gamma = p->gamma;
@@ -169,7 +184,6 @@ extern "C" int mhd3d_cfl_noalloc(const mhd3d_params* p,
     s.npx = p->npx;
     s.npy = p->npy;
     s.npz = p->npz;
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
     auto* part = static_cast<unsigned long long*>(partials);
     if (p->lmag)
         noalloc::k_cfl_planes<true><<<p->npz, noalloc::NTHR, 0, cs>>>(s, ru, rv, rw, tt, ro, bx, by, bz, ddx, ddy, ddz,

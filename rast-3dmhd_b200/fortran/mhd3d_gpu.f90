@@ -2,8 +2,8 @@
 ! (include/mhd3d.h) for the reference's Fortran driver.
 !
 ! The driver keeps its COMMON blocks and calls these routines in place of
-! CALL STEP (3dmhd.f:912); see INTEGRATION.md for the patch.  The derived
-! type mirrors struct mhd3d_params field for field.
+! CALL STEP (3dmhd.f:912).  The derived type mirrors struct mhd3d_params
+! field for field.
 module mhd3d_gpu
   use, intrinsic :: iso_c_binding
   implicit none
@@ -85,5 +85,18 @@ module mhd3d_gpu
        type(c_ptr), value :: handle
        real(c_double), intent(out) :: prof(*)
      end function mhd3d_profiles
+
+     ! CFL/Mach reduction that allocates nothing, for hosts whose device
+     ! arrays are declared statically: every array argument is a device
+     ! address (c_loc of a device array), out receives DT, UMACH and the
+     ! non-finite flag on the device, stream is a cudaStream_t or c_null_ptr
+     integer(c_int) function mhd3d_cfl_noalloc(p, ru, rv, rw, tt, ro, bx, by, bz, ddx, ddy, ddz, rkapa, &
+          out, stream) bind(C, name="mhd3d_cfl_noalloc")
+       import :: c_int, c_ptr, mhd3d_params
+       type(mhd3d_params), intent(in) :: p
+       type(c_ptr), value :: ru, rv, rw, tt, ro, bx, by, bz
+       type(c_ptr), value :: ddx, ddy, ddz, rkapa
+       type(c_ptr), value :: out, stream
+     end function mhd3d_cfl_noalloc
   end interface
 end module mhd3d_gpu

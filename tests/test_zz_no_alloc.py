@@ -61,6 +61,40 @@ def test_noalloc_cfl_matches_handle_twice(mhd3d):
     sim.close()
 
 
+def test_noalloc_cfl_hydro_and_nonfinite_flag(mhd3d):
+    """The lmag=0 form (B pointers NULL) equals mhd3d_cfl bit for bit, and a
+    NaN in one interior cell raises the non-finite flag."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a CUDA device")
+    cfg = mhd3d.convection_config(36, 20, 16, ra=1e6, ta=1e6)
+    cfg.lmag = 0
+    setup = mhd3d.make_setup(cfg)
+    assert setup.params.lmag == 0 and setup.state["bx"] is None
+    sim = mhd3d.GpuSim(setup, mode=mhd3d.MODE_EXACT)
+    sim.upload(setup.state)
+    sim.step(2)
+    dt, um = sim.cfl()
+    state = sim.download()
+    sim.close()
+    out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(-1.0)
+        assert _call(mhd3d, torch, setup.params, state, setup.grid, out) == 0
+        got = out.cpu().numpy()
+        assert got[0] == dt and got[1] == um and got[2] == 0.0
+    bad = {f: (None if v is None else v.copy(order="F")) for f, v in state.items()}
+    bad["tt"][7, 5, 9] = np.nan
+    out.fill_(-1.0)
+    assert _call(mhd3d, torch, setup.params, bad, setup.grid, out) == 0
+    assert out.cpu().numpy()[2] == 1.0
+    # and the next call on a finite state clears it again
+    out.fill_(-1.0)
+    assert _call(mhd3d, torch, setup.params, state, setup.grid, out) == 0
+    got = out.cpu().numpy()
+    assert got[0] == dt and got[1] == um and got[2] == 0.0
+
+
 def test_noalloc_rejects_more_planes_than_its_scratch(mhd3d):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
