@@ -373,12 +373,14 @@ def run_ensemble(args, rank, world, local):
     return 0
 
 
-def run_closure(args, rank, world, local):
+def closure_measure(args, rank, world, local, dt_fine=None):
     """The coarse side of the headline comparison: 128x128x64 FP32 with the
     learned closure attached (evaluated every step: features, three tcgen05
-    convolutions, tendencies), same physics as the fine workload.  Also
-    reports the fine-equivalent rate 512^2*256 * (DT_coarse/DT_fine) /
-    wall, which assumes the closure holds the fine run's flux error."""
+    convolutions, tendencies), same physics as the fine workload, timed with
+    CUDA events on its stream; the fine-equivalent rate 512^2*256 *
+    (DT_coarse/DT_fine) / wall; and the tensor roofline of the three
+    convolutions of one evaluation timed alone.  Returns the pieces for a
+    bench line (the handle stays open for the e2e pass of run_closure)."""
     import torch
     import mhd3d
     import closure
@@ -411,14 +413,15 @@ def run_closure(args, rank, world, local):
     clk = clocks.stop() if clocks else None
     status = sim.closure_status()
     value = world * cells * args.steps / (ms / 1e3) / 1e6
-    # DT of the fine 512x512x256 run from the same initial physics (one CFL pass)
-    fcfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"], w["contrast"],
-                                   w["m"], w["beta"], w["stretch"], w["ampt"], seed=62659 + rank)
-    fsetup = mhd3d.make_setup(fcfg)
-    fine = mhd3d.GpuSim(fsetup, mode=mhd3d.MODE_FAST)
-    fine.upload(fsetup.state)
-    dt_fine, _ = fine.cfl()
-    fine.close()
+    if dt_fine is None:
+        # DT of the fine 512x512x256 run from the same initial physics (one CFL pass)
+        fcfg = mhd3d.convection_config(w["npx"], w["npy"], w["npz"], w["ra"], w["ta"], w["pr"], w["pm"],
+                                       w["contrast"], w["m"], w["beta"], w["stretch"], w["ampt"], seed=62659 + rank)
+        fsetup = mhd3d.make_setup(fcfg)
+        fine = mhd3d.GpuSim(fsetup, mode=mhd3d.MODE_FAST)
+        fine.upload(fsetup.state)
+        dt_fine, _ = fine.cfl()
+        fine.close()
     dt_coarse = res["dt"]
     fine_cells = w["npx"] * w["npy"] * w["npz"]
     fine_equiv = fine_cells * (dt_coarse / dt_fine) * args.steps / (ms / 1e3) / 1e6
@@ -467,6 +470,48 @@ def run_closure(args, rank, world, local):
             "algorithmic_flop_per_evaluation": alg_flop, "ms_per_evaluation": conv_ms,
             "peak_source": "measured MEASURED_PEAKS.json bf16_tflops (burst)" if peak_kind == "measured"
             else "fallback 1.59 PFLOP/s"}
+    return {"sim": sim, "setup": setup, "cfg": cfg, "stream": stream, "cells": cells, "ms": ms, "value": value,
+            "status": status, "dt_coarse": dt_coarse, "dt_fine": dt_fine, "fine_equiv": fine_equiv, "roof": roof,
+            "clocks": clk}
+
+
+def closure_profile_record():
+    """The a-posteriori profile errors of the closure case as last measured by
+    rast-3dmhd_b200/closure_case.py (grid sizes named in the record), read
+    from its committed summary; None when the summary is absent."""
+    path = os.path.join(ROOT, "profiles", "closure_case_profile_errors.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def closure_summary(args, rank, world, local, dt_fine):
+    """The closure object of the default line: the coarse FP32+closure rate
+    measured here, its fine-equivalent rate, the convolutions' tensor
+    roofline, and the recorded profile errors of the closure case."""
+    cm = closure_measure(args, rank, world, local, dt_fine=dt_fine)
+    cm["sim"].close()
+    return {"workload": "FP32+closure coarse run, 128x128x64, same physics as the fine workload, closure evaluated "
+                        "every step (network weights seeded, not trained: throughput does not depend on them)",
+            "value": cm["value"], "unit": UNIT, "ms_per_step": cm["ms"] / args.steps, "steps": args.steps,
+            "dt_coarse": cm["dt_coarse"], "dt_fine": cm["dt_fine"],
+            "fine_equivalent_value": cm["fine_equiv"],
+            "fine_equivalent_formula": "512^2*256 cells x (DT_coarse/DT_fine) x steps / coarse wall",
+            "closure_status": cm["status"], "conv_roofline": cm["roof"],
+            "profile_error": closure_profile_record()}
+
+
+def run_closure(args, rank, world, local):
+    """The FP32+closure coarse run as its own bench line (see closure_measure),
+    with an e2e pass through the C-ABI."""
+    import torch
+    import mhd3d
+
+    cm = closure_measure(args, rank, world, local)
+    sim, setup, cfg, stream, cells = cm["sim"], cm["setup"], cm["cfg"], cm["stream"], cm["cells"]
+    ms, value, status, roof, clk = cm["ms"], cm["value"], cm["status"], cm["roof"], cm["clocks"]
+    dt_coarse, dt_fine, fine_equiv = cm["dt_coarse"], cm["dt_fine"], cm["fine_equiv"]
 
     # end to end through the C-ABI: upload from pinned memory, K steps with
     # the closure, download
@@ -529,6 +574,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-compare", action="store_true",
                     help="only time the CPU baselines (oracle at 1 and all threads, translated reference)")
+    ap.add_argument("--no-closure", action="store_true",
+                    help="skip the FP32+closure coarse measurement of the default line")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end pass (it pins two host copies of the state)")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -708,8 +755,14 @@ def main():
                            "last_dt": res["dt"], "nit": res["nit"]},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 4 * args.steps, "clocks": clk}
-        print(json.dumps(line), flush=True)
     sim.close()
+    # the metric's other half: the FP32+closure coarse run (default workload only)
+    if not args.case and not args.grid and not args.no_closure:
+        summary = closure_summary(args, rank, world, local, dt_fine=res["dt"])
+        if rank == 0:
+            line["closure"] = summary
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

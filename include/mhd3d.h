@@ -214,32 +214,46 @@ int mhd3d_sync(void* handle, double* dt, double* timc, double* timt, double* uma
  * (after mhd3d_sync) returns the summed milliseconds and launch counts of
  * stages 1, 2, 3 since the last read, then clears them.
  */
+/*
+ * Test entry point (no counterpart in the reference, whose only run-time
+ * check is DT<1e-8, 3dmhd.f:924): the poll limit of the first wait of every
+ * CTA of the FP64 stage kernels on its shared-memory ring (default and
+ * maximum 2^22 polls).  With 0 that wait gives up at once; the CTA then
+ * waits, at the normal limit, for every copy it has in flight, records
+ * MHD3D_ERR_TIMEOUT and returns, so the next mhd3d_step reports the
+ * timeout the way a real expiry would.  Returns MHD3D_ERR_ARG for an FP32
+ * handle or a negative limit.
+ */
+int mhd3d_set_wait_limit(void* handle, int64_t polls);
 int mhd3d_profile(void* handle, int32_t enable);
 int mhd3d_profile_read(void* handle, double stage_ms[3], int32_t launches[3]);
 
 /*
- * CFL/Mach reduction that allocates nothing.  No counterpart in the
+ * CFL/Mach reduction that allocates nothing.  It has no counterpart in the
  * reference: it serves hosts that cannot call cudaMalloc (device arrays
  * declared statically by a Fortran or C code, a framework allocator that
  * owns the device heap, a hard device-memory cap) and already hold the
  * state in device memory.
  *
  * Inputs are device pointers: the fields as Fortran (NX,NY,NZ) arrays
- * (bx/by/bz only with lmag), and DDX(NX), DDY(NY), DDZ(NZ), RKAPA(NZ).
- * out is a device pointer to 3 doubles: DT = SF*MIN(limits), UMACH, and
- * 1.0 if any limit was not finite (else 0.0), as STEP computes them
- * (3dmhdsub.f:741-873) and as mhd3d_cfl returns them in the
- * reference-rounding mode.  The work is enqueued on stream (a cudaStream_t,
- * NULL for the default stream) and the call returns without waiting.
+ * (bx/by/bz only with lmag; NULL otherwise), and DDX(NX), DDY(NY), DDZ(NZ),
+ * RKAPA(NZ).  out is a device pointer to 3 doubles: DT = SF*MIN(limits),
+ * UMACH, and 1.0 if any limit was not finite (else 0.0), equal bit for bit
+ * to what mhd3d_cfl returns in the reference-rounding mode.  The work is
+ * enqueued on stream (a cudaStream_t, NULL for the default stream) and the
+ * call returns without waiting.
  *
  * Scratch: one file-scope __device__ array of MHD3D_NOALLOC_MAX_PLANES x 6
  * 64-bit words (192 KiB), held by every GPU that loads the library until
  * the process exits; npz above MHD3D_NOALLOC_MAX_PLANES returns
- * MHD3D_ERR_ARG.  The first call on a device looks the array's device
- * address up on that device, so make that first call before any CUDA graph
- * capture.  All calls share the array and keep the last call's contents:
- * calls that can overlap on the GPU (different streams, or devices sharing
- * a context) race and must be ordered by the caller.
+ * MHD3D_ERR_ARG.  Each call made outside a stream capture looks the array's
+ * device address up on the current device (so a cudaDeviceReset between
+ * calls is harmless); a call made while its stream is being captured reuses
+ * the address found by the last such call on that device, so make the first
+ * call on a device before any stream capture.  All calls share the array
+ * and keep the last call's contents: calls that can overlap on the GPU
+ * (different streams, or devices sharing a context) race and must be
+ * ordered by the caller.
  */
 #define MHD3D_NOALLOC_MAX_PLANES 4096
 int mhd3d_cfl_noalloc(const mhd3d_params* p,
@@ -264,9 +278,14 @@ int mhd3d_cfl_noalloc(const mhd3d_params* p,
  * nsteps steps of every member without waiting; mhd3d_ensemble_sync waits
  * and returns per-member DT, TIMT, NIT and status (arrays of nmembers; any
  * may be NULL) and the first non-zero status.  mhd3d_ensemble_tune times
- * `steps` steps for each z-chunk length in {4,6,8,12,16,24,32,48,64} and
- * persistent CTAs per SM in {2,3,4} on the current state, restores the
- * state, and keeps the fastest pair.
+ * `steps` steps for each tile shape (32x2, 32x4, 32x8 columns; separate
+ * kernel instances, each member's TMA boxes re-made for it), z-chunk length
+ * in {4,6,8,12,16,24,32,48,64} and number of persistent CTAs per SM (8, 12
+ * or 16 warps an SM where the tile allows) on the current state, restores
+ * the state, and keeps the fastest; mhd3d_ensemble_tile reports the tile
+ * shape in use (32x4 until a tune), mhd3d_ensemble_set_tile sets its rows
+ * (2, 4 or 8; MHD3D_ERR_ARG for others or rows a member's arrays cannot
+ * hold).  Every tile shape gives the same bits.
  */
 int mhd3d_ensemble_create(int32_t nmembers, const mhd3d_params* params, const double* const* grids, void** ens);
 int mhd3d_ensemble_destroy(void* ens);
@@ -274,6 +293,8 @@ int mhd3d_ensemble_member(void* ens, int32_t i, void** handle);
 int mhd3d_ensemble_step(void* ens, int32_t nsteps);
 int mhd3d_ensemble_sync(void* ens, double* dt, double* timt, int32_t* nit, int32_t* status);
 int mhd3d_ensemble_tune(void* ens, int32_t steps, int32_t* zlen, int32_t* ctas_per_sm, double* ms_per_step);
+int mhd3d_ensemble_tile(void* ens, int32_t* tile_x, int32_t* tile_y);
+int mhd3d_ensemble_set_tile(void* ens, int32_t tile_y);
 /* enqueue the ensemble's work on a caller's cudaStream_t (NULL: its own) */
 int mhd3d_ensemble_set_stream(void* ens, void* stream);
 
@@ -293,7 +314,11 @@ int mhd3d_ensemble_set_stream(void* ens, void* stream);
  * mhd3d_conv3d_wtranspose: w -> wt, the weights of the input-gradient
  * convolution (cin and cout swapped, taps mirrored).
  * mhd3d_conv3d_wgrad: dw[cout][27*cin] += sum over voxels of dy (x) x
- * shifted, db[cout] += sum of dy (FP32, accumulating).
+ * shifted, db[cout] += sum of dy (FP32, accumulating), on the tensor cores
+ * with FP32 accumulation; per-CTA partial sums go to a workspace taken from
+ * the stream-ordered allocator (cudaMallocAsync on stream, freed after use)
+ * and are added in a fixed order, so repeated calls give the same bits.  If
+ * a bounded device-side wait gives up, dw and db receive NaN.
  */
 int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const float* bias, const void* mask,
                  int32_t relu, void* y, float* yf, int32_t nx, int32_t ny, int32_t nz, int32_t* err, void* stream);

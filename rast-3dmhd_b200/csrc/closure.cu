@@ -21,9 +21,12 @@
 //    MMA thread and four epilogue warps, handing off through mbarriers.  The
 //    epilogue adds the bias, applies ReLU or the ReLU mask of the layer
 //    below, and writes BF16 (and FP32) outputs.
-//  - k_conv3d_wgrad: dW[n][tap*CIN+ci] = sum over voxels of dY[v][n] *
-//    X[v+tap][ci], an FP32 CUDA-core reduction (its M = COUT is below the
-//    64 rows of a tcgen05 instruction and its K runs over all voxels).
+//  - k_conv3d_wgrad_tc: dW[n][tap*CIN+ci] = sum over voxels of dY[v][n] *
+//    X[v+tap][ci] on tcgen05 as well, with K running over voxels: per x
+//    segment the shifted dY rows form A (M = 3*COUT, the x taps) and the
+//    input rows of the y taps form B (N = 3*CIN, the z taps), both staged
+//    K-major by the CTA's threads; per-CTA partials are added in CTA order
+//    by k_wgrad_reduce.
 //
 // Every wait is bounded; a CTA that gives up records an error and releases
 // its tensor memory.
@@ -46,7 +49,6 @@ constexpr int CT = 32 * (4 + NLW + 1);   // threads: 4 epilogue warps (TMEM lane
 constexpr int RING = 4;            // input rows held in the ring: the loaders run up to three steps ahead
 constexpr int MT = 128;            // output voxels per tile: one 128-point x segment
 constexpr int BX = MT + 2;         // input block: x with halo
-constexpr int VB = BX * 3 * 3;     // voxels of the input block (y, z halos)
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -118,32 +120,6 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Issue the asynchronous copies of the input block of tile (x0, y, z) into sx:
-// [chunk][voxel] 16-byte rows, periodic in x and y, zeros outside in z (a
-// zero-byte source fills zeros).  The caller commits and waits for the group.
-template <int CIN, int NTH>
-__device__ __forceinline__ void load_block_async(unsigned char* sx, const __nv_bfloat16* __restrict__ x, int x0,
-                                                 int y, int z, int nx, int ny, int nz)
-{
-    constexpr int NC = CIN / 8;
-    const uint32_t sbase = smem_u32(sx);
-    for (int q = threadIdx.x; q < VB * NC; q += NTH) {
-        const int c = q / VB, v = q % VB;
-        const int xi = v % BX, yi = (v / BX) % 3, zi = v / (BX * 3);
-        int gx = x0 - 1 + xi;
-        if (nx >= MT) gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
-        else gx = (gx + nx) % nx;   // a 128-point tile spans 128/nx periods
-        int gy = y - 1 + yi;
-        gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
-        int gz = z - 1 + zi;
-        const uint32_t nbytes = (gz >= 0 && gz < nz) ? 16u : 0u;
-        gz = gz < 0 ? 0 : (gz >= nz ? nz - 1 : gz);
-        const __nv_bfloat16* src = x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sbase + (uint32_t)((c * VB + v) * 16)),
-                     "l"(src), "r"(nbytes)
-                     : "memory");
-    }
-}
 // Ring of input rows for the convolution: [chunk][slot 0..RING-1][z plane 0..2]
 // [BXP] of 16-byte rows (or, in the swizzled form, [slot][z plane][BXP] of
 // 64-byte rows), voxel xi (x0-1+xi) at row XR0+xi, so that the 128 interior
@@ -617,62 +593,276 @@ __global__ void __launch_bounds__(CT, 1) k_conv3d(const __grid_constant__ CUtens
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::NCOL));
 }
 
-// dW[n][tap*CIN+ci] += sum_v dY[v][n] * X[v+tap][ci], db[n] += sum_v dY[v][n].
-// Thread t owns output channel n = t/(CIN/4) and input channels 4*(t%(CIN/4))..+3.
+// ---------------------------------------------------------------------------
+// Weight gradient on the tensor cores.
+//
+// dW[n][tap(dx,dy,dz)*CIN+ci] = sum_v dY[v][n] X[v + (dx-1, dy-1, dz-1)][ci]
+// is a GEMM whose K runs over voxels.  For an x segment of WT=64 voxels
+// (x0..x0+63) of one (y, z) row, with u = 0..KT-1 indexing x0-1+u:
+//
+//   A[(dx, n)][u]   = dY[x0 + u - dx][n]  (zero outside the segment's own
+//                     voxels; rows 3*COUT..127 zero)           M = 128
+//   B_dy[(dz,ci)][u] = X[x0-1+u, y+dy-1, z+dz-1][ci] (periodic in x, y; zero
+//                     outside z and for u >= WT+2)             N = 3*CIN
+//   D_dy[(dx,n)][(dz,ci)] += sum_u A B_dy                      K = KT = 80
+//
+// so one segment is 3 (y taps) x 5 (K steps of 16) MMAs of M=128, N=3*CIN,
+// both operands K-major in the canonical no-swizzle layout, staged by the
+// CTA's threads: A from a transposed copy of the segment's dY (the x tap is
+// a shift by 0..2 elements, formed with byte permutes), B by 8x8 transposes
+// of the channels-last input.  Segments alternate between two staging
+// buffers, so the MMAs of one overlap the staging of the next.  The three
+// accumulators (3*3*CIN columns) stay in TMEM over all of a CTA's segments
+// (a fixed set, in a fixed order); each CTA writes its partial sums to a
+// workspace row and a second kernel adds the rows to dW in CTA order, so the
+// result does not depend on timing.
+constexpr int WT = 64;               // voxels of an x segment
+constexpr int KT = 80;               // K of a segment: WT + 2 halo voxels, padded to 16
+constexpr int WG_NTH = 256;          // threads of a weight-gradient CTA
+constexpr int DYW = 8 + KT + 8;      // row of the transposed dY: 8 zeros, the segment, zeros
+
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(COUT * CIN / 4) k_conv3d_wgrad(const __nv_bfloat16* __restrict__ x,
-                                                                const __nv_bfloat16* __restrict__ dy,
-                                                                float* __restrict__ dw, float* __restrict__ db, int nx,
-                                                                int ny, int nz)
+struct WgLay {
+    static constexpr int N = 3 * CIN;                         // columns of one y-tap accumulator
+    static constexpr uint32_t NCOL = 3 * N <= 256 ? 256 : 512;
+    static constexpr size_t A_B = (size_t)(KT / 8) * 128 * 16;    // one A buffer
+    static constexpr size_t BD_B = (size_t)(KT / 8) * N * 16;     // one y tap of a B buffer
+    static constexpr size_t B_B = 3 * BD_B;
+    static constexpr size_t BUF_B = A_B + B_B;
+    static constexpr size_t DYT_OFF = 2 * BUF_B;
+    static constexpr size_t DYT_B = (size_t)COUT * DYW * 2;
+    static constexpr size_t RED_OFF = (DYT_OFF + DYT_B + 15) / 16 * 16;
+    static constexpr size_t RED_B = (size_t)WG_NTH * 8 * 4;
+    static constexpr size_t BAR_OFF = RED_OFF + RED_B;
+    static constexpr size_t BYTES = BAR_OFF + 2 * 8 + 16 + 1024;   // + alignment of the base to 1024 bytes
+};
+
+// 8x8 transpose of BF16: v[a] holds 8 channels of voxel a (word w: channels
+// 2w, 2w+1); r[i] receives voxels 0..7 of channel i
+__device__ __forceinline__ void transpose8(const uint4 (&v)[8], uint4 (&r)[8])
 {
-    constexpr int NTH = COUT * CIN / 4;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t sel = (i & 1) ? 0x7632u : 0x5410u;
+        uint32_t o[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const uint4& a = v[2 * w];
+            const uint4& b = v[2 * w + 1];
+            const uint32_t wa = (i >> 1) == 0 ? a.x : (i >> 1) == 1 ? a.y : (i >> 1) == 2 ? a.z : a.w;
+            const uint32_t wb = (i >> 1) == 0 ? b.x : (i >> 1) == 1 ? b.y : (i >> 1) == 2 ? b.z : b.w;
+            o[w] = __byte_perm(wa, wb, sel);
+        }
+        r[i] = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(WG_NTH, 1) k_conv3d_wgrad_tc(const __nv_bfloat16* __restrict__ x,
+                                                               const __nv_bfloat16* __restrict__ dy,
+                                                               float* __restrict__ ws, int nx, int ny, int nz,
+                                                               int* __restrict__ err)
+{
+    using L = WgLay<CIN, COUT>;
+    constexpr int N = L::N, K = 27 * CIN, NCC = CIN / 8, NNC = COUT / 8;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* const sx = smem_raw;                              // CIN/8 x VB x 16 B
-    float* const sdy = reinterpret_cast<float*>(smem_raw + (size_t)CIN * VB * 2);   // MT x COUT
-    const int tid = threadIdx.x;
-    const int n = tid / (CIN / 4), c4 = tid % (CIN / 4);
-    float acc[27][4];
-#pragma unroll
-    for (int t = 0; t < 27; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
-    float bacc = 0.f;
-    const int nseg = (nx + MT - 1) / MT;
+    unsigned char* const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    __nv_bfloat16* const dyt = reinterpret_cast<__nv_bfloat16*>(sb + L::DYT_OFF);
+    float* const red = reinterpret_cast<float*>(sb + L::RED_OFF);
+    unsigned long long* const mmadone = reinterpret_cast<unsigned long long*>(sb + L::BAR_OFF);
+    uint32_t* const tslot = reinterpret_cast<uint32_t*>(sb + L::BAR_OFF + 16);
+    volatile int* const abort_flag = reinterpret_cast<volatile int*>(sb + L::BAR_OFF + 20);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // A rows 3*COUT..127 stay zero in both buffers; the dY padding is rewritten per segment
+    for (int q = tid; q < 2 * (KT / 8) * 128; q += WG_NTH) {
+        const int b = q / ((KT / 8) * 128), r = q % ((KT / 8) * 128);
+        const int row = r % 128, kc = r / 128;
+        if (row >= 3 * COUT)
+            *reinterpret_cast<uint4*>(sb + b * L::BUF_B + (size_t)kc * 2048 + row * 16) = make_uint4(0, 0, 0, 0);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(L::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(mmadone + 0, 1);
+        mbar_init(mmadone + 1, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    const int nseg = (nx + WT - 1) / WT;
     const int ntile = nseg * ny * nz;
-    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    float dbacc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // dY sums of this thread's 8 channels
+    int i = 0;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x, ++i) {
         const int seg = t % nseg, yy = (t / nseg) % ny, zz = t / (nseg * ny);
-        const int x0 = seg * MT;
+        const int x0 = seg * WT;
+        const int mlim = nx - x0 < WT ? nx - x0 : WT;   // the segment's own voxels (nx < 64: one period)
+        const int b = i & 1;
+        unsigned char* const sa = sb + b * L::BUF_B;
+        unsigned char* const sbb = sa + L::A_B;
+        // the buffer was last read by the MMAs of segment i-2
+        if (i >= 2) {
+            bool ok = true;
+            if (tid == 0) ok = mbar_wait(mmadone + b, (unsigned)((i - 2) >> 1) & 1u);
+            if (!ok) *abort_flag = 1;
+        }
         __syncthreads();
-        load_block_async<CIN, NTH>(sx, x, x0, yy, zz, nx, ny, nz);
-        cp_async_commit();
-        const size_t row = ((size_t)zz * ny + yy) * nx + x0;
-        const int mlim = nx - x0 < MT ? nx - x0 : MT;   // voxels of this tile that are the row's own
-        for (int q = threadIdx.x; q < mlim * COUT; q += NTH) sdy[q] = __bfloat162float(dy[row * COUT + q]);
-        cp_async_wait<0>();
-        __syncthreads();
-        // channels 4*c4..4*c4+3 live in chunk c4/2, halves (c4%2)
-        const unsigned char* xb = sx + (size_t)(c4 >> 1) * VB * 16 + (c4 & 1) * 8;
-        for (int m = 0; m < mlim; ++m) {
-            const float g = sdy[m * COUT + n];
-            bacc += g;
+        if (*abort_flag) break;
+        // ---- dY of the segment, transposed: dyt[n][8 + j], zeros around it
+        {
+            const size_t row = ((size_t)zz * ny + yy) * nx + x0;
+            for (int q = tid; q < WT * NNC; q += WG_NTH) {
+                const int nc = q % NNC, j = q / NNC;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (j < mlim) v = __ldg(reinterpret_cast<const uint4*>(dy + (row + j) * COUT + nc * 8));
+                const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-            for (int tap = 0; tap < 27; ++tap) {
-                const int v = m + (tap % 3) + BX * ((tap / 3) % 3) + BX * 3 * (tap / 9);
-                const uint2 p = *reinterpret_cast<const uint2*>(xb + (size_t)v * 16);
-                const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&p.x);
-                const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&p.y);
-                const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
-                acc[tap][0] += g * fa.x;
-                acc[tap][1] += g * fa.y;
-                acc[tap][2] += g * fb.x;
-                acc[tap][3] += g * fb.y;
+                for (int e = 0; e < 8; ++e) {
+                    dyt[(nc * 8 + e) * DYW + 8 + j] = h[e];
+                    dbacc[e] += __bfloat162float(h[e]);
+                }
+            }
+            for (int q = tid; q < COUT * 16; q += WG_NTH) {
+                const int n = q / 16, e = q % 16;
+                dyt[n * DYW + (e < 8 ? e : 8 + WT + (e - 8))] = __float2bfloat16_rn(0.f);
+            }
+            for (int q = tid; q < COUT * (KT - WT); q += WG_NTH) {   // beyond the segment up to KT
+                const int n = q / (KT - WT), e = q % (KT - WT);
+                if (8 + WT + 8 + e < DYW) dyt[n * DYW + 8 + WT + 8 + e] = __float2bfloat16_rn(0.f);
             }
         }
+        __syncthreads();
+        // ---- A[(dx, n)][u] = dyt[n][8 + u - dx]: 16-byte rows (kc, row)
+        for (int q = tid; q < (KT / 8) * 3 * COUT; q += WG_NTH) {
+            const int kc = q / (3 * COUT), m = q % (3 * COUT);
+            const int dxs = m / COUT, n = m % COUT;
+            const uint4 c0 = *reinterpret_cast<const uint4*>(dyt + n * DYW + kc * 8);       // elements 8kc-8 ..
+            const uint4 c1 = *reinterpret_cast<const uint4*>(dyt + n * DYW + kc * 8 + 8);   // elements 8kc ..
+            uint4 o;
+            if (dxs == 0) o = c1;
+            else if (dxs == 2) o = make_uint4(c0.w, c1.x, c1.y, c1.z);
+            else o = make_uint4(__byte_perm(c0.w, c1.x, 0x5432), __byte_perm(c1.x, c1.y, 0x5432),
+                                __byte_perm(c1.y, c1.z, 0x5432), __byte_perm(c1.z, c1.w, 0x5432));
+            *reinterpret_cast<uint4*>(sa + (size_t)kc * 2048 + m * 16) = o;
+        }
+        // ---- B_dy[(dz, ci)][u]: 8x8 transposes of the input rows
+        for (int q = tid; q < 9 * NCC * (KT / 8); q += WG_NTH) {
+            const int kc = q % (KT / 8), c = (q / (KT / 8)) % NCC, rz = q / ((KT / 8) * NCC);
+            const int dys = rz / 3, dzs = rz % 3;
+            int gy = yy + dys - 1;
+            gy = gy < 0 ? gy + ny : (gy >= ny ? gy - ny : gy);
+            const int gz = zz + dzs - 1;
+            uint4 v[8];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const int u = kc * 8 + a;
+                v[a] = make_uint4(0, 0, 0, 0);
+                if (gz >= 0 && gz < nz && u < WT + 2) {
+                    int gx = x0 - 1 + u;
+                    if (nx >= WT) gx = gx < 0 ? gx + nx : (gx >= nx ? gx - nx : gx);
+                    else gx = (gx + nx) % nx;
+                    v[a] = __ldg(reinterpret_cast<const uint4*>(x + (((size_t)gz * ny + gy) * nx + gx) * CIN + c * 8));
+                }
+            }
+            uint4 r[8];
+            transpose8(v, r);
+            unsigned char* dst = sbb + (size_t)dys * L::BD_B + (size_t)kc * (N * 16) + (size_t)(dzs * CIN + c * 8) * 16;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) *reinterpret_cast<uint4*>(dst + e * 16) = r[e];
+        }
+        fence_proxy_async();   // plain stores above are read by the tensor cores
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            constexpr uint32_t IDESC = idesc_bf16(128, N);
+            const uint32_t aaddr = smem_u32(sa), baddr = smem_u32(sbb);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int k2 = 0; k2 < KT / 16; ++k2) {
+                    const uint64_t da = smem_desc(aaddr + (uint32_t)(2 * k2) * 2048u, 2048u, 128u);
+                    const uint64_t db = smem_desc(baddr + (uint32_t)(d * L::BD_B + (size_t)(2 * k2) * N * 16),
+                                                  (uint32_t)(N * 16), 128u);
+                    umma_bf16(tmem + (uint32_t)(d * N), da, db, IDESC, (i == 0 && k2 == 0) ? 0u : 1u);
+                }
+            umma_commit(mmadone + b);
+        }
     }
-    constexpr int K = 27 * CIN;
+    // every MMA issued has completed once the last commit of each buffer has
+    const int nmine = i;
+    if (tid == 0) {
+        for (int j = nmine - 2 < 0 ? 0 : nmine - 2; j < nmine; ++j)
+            if (!mbar_wait(mmadone + (j & 1), (unsigned)(j >> 1) & 1u)) *abort_flag = 1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    float* const wrow = ws + (size_t)blockIdx.x * ((size_t)COUT * K + COUT);
+    if (*abort_flag) {
+        if (tid == 0) atomicExch(err, 1);
+    } else if (nmine > 0 && warp < 4) {
+        // accumulator lane m = (dx, n); columns (dz, ci) of y tap d
+        const int m = warp * 32 + lane;
+        const int dxs = m / COUT, n = m % COUT;
 #pragma unroll
-    for (int tap = 0; tap < 27; ++tap)
+        for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) atomicAdd(&dw[(size_t)n * K + tap * CIN + 4 * c4 + i], acc[tap][i]);
-    if (c4 == 0 && db) atomicAdd(&db[n], bacc);
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tmem_ld<16>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * N + c0), v);
+                if (dxs < 3) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int col = c0 + e, dzs = col / CIN, ci = col % CIN;
+                        wrow[(size_t)n * K + (dxs + 3 * d + 9 * dzs) * CIN + ci] = v[e];
+                    }
+                }
+            }
+    } else if (nmine == 0 && warp < 4) {
+        // a CTA without segments contributes zeros
+        for (int q = tid; q < COUT * K; q += 128) wrow[q] = 0.f;
+    }
+    // bias gradient: this thread's 8 channel sums, added up over the threads
+    // that hold the same channels, in thread order
+#pragma unroll
+    for (int e = 0; e < 8; ++e) red[tid * 8 + e] = dbacc[e];
+    __syncthreads();
+    if (tid < COUT) {
+        const int nc = tid / 8, e = tid % 8;
+        float sacc = 0.f;
+        for (int t2 = nc; t2 < WG_NTH; t2 += NNC) sacc += red[t2 * 8 + e];
+        wrow[(size_t)COUT * K + tid] = sacc;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::NCOL));
+}
+
+// dW += sum over CTAs of their rows of the workspace, in CTA order (and db);
+// NaN everywhere when a CTA of the gradient kernel gave up a wait
+__global__ void k_wgrad_reduce(const float* __restrict__ ws, int rows, int nw, int nb, float* __restrict__ dw,
+                               float* __restrict__ db, const int* __restrict__ err)
+{
+    const int stride = nw + nb;
+    const bool bad = *err != 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < stride; q += gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int r = 0; r < rows; ++r) acc += ws[(size_t)r * stride + q];
+        if (bad) acc = __int_as_float(0x7fc00000);
+        if (q < nw) dw[q] += acc;
+        else if (db) db[q - nw] += acc;
+    }
 }
 
 // W[n][tap*CIN+ci] -> Wt[ci][(26-tap)*COUT+n]: the input-gradient convolution
@@ -747,21 +937,43 @@ cudaError_t launch_conv_t(const void* x, const void* w, const float* bias, const
     return cudaGetLastError();
 }
 
+// the tensor-core weight gradient: one CTA per SM (a fixed grid of at most
+// the SM count over the segments), its partial rows in a stream-ordered
+// workspace, then the ordered reduction into dw, db
 template <int CIN, int COUT>
-cudaError_t launch_wgrad_t(const void* x, const void* dy, float* dw, float* db, int nx, int ny, int nz, cudaStream_t st)
+cudaError_t launch_wgrad_tc_t(const void* x, const void* dy, float* dw, float* db, int nx, int ny, int nz,
+                              cudaStream_t st)
 {
-    const size_t smem = (size_t)CIN * VB * 2 + (size_t)MT * COUT * 4;
+    using L = WgLay<CIN, COUT>;
     static std::atomic<unsigned long long> attr{0};
-    cudaError_t ae = smem_attr_once(attr, reinterpret_cast<const void*>(k_conv3d_wgrad<CIN, COUT>), smem);
+    cudaError_t ae = smem_attr_once(attr, reinterpret_cast<const void*>(k_conv3d_wgrad_tc<CIN, COUT>), L::BYTES);
     if (ae != cudaSuccess) return ae;
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ntile = ((nx + MT - 1) / MT) * ny * nz;
-    const int grid = ntile < 2 * sms ? ntile : 2 * sms;
-    k_conv3d_wgrad<CIN, COUT><<<grid, COUT * CIN / 4, smem, st>>>(
-        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, db, nx, ny, nz);
-    return cudaGetLastError();
+    const int ntile = ((nx + WT - 1) / WT) * ny * nz;
+    const int grid = ntile < sms ? ntile : sms;
+    const size_t stride = (size_t)COUT * 27 * CIN + COUT;
+    const size_t bytes = (size_t)grid * stride * sizeof(float) + 16;
+    void* buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, bytes, st);
+    if (e != cudaSuccess) return e;
+    int* err = reinterpret_cast<int*>(static_cast<char*>(buf) + (size_t)grid * stride * sizeof(float));
+    e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+        k_conv3d_wgrad_tc<CIN, COUT><<<grid, WG_NTH, L::BYTES, st>>>(
+            static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), static_cast<float*>(buf),
+            nx, ny, nz, err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        const int nw = COUT * 27 * CIN;
+        k_wgrad_reduce<<<(int)((stride + 255) / 256), 256, 0, st>>>(static_cast<const float*>(buf), grid, nw, COUT,
+                                                                    dw, db, err);
+        e = cudaGetLastError();
+    }
+    const cudaError_t f = cudaFreeAsync(buf, st);
+    return e != cudaSuccess ? e : f;
 }
 
 }  // namespace clo
@@ -796,9 +1008,9 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
     if (!aligned16(x) || !aligned16(dy)) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;
-    if (cin == 16 && cout == 32) e = launch_wgrad_t<16, 32>(x, dy, dw, db, nx, ny, nz, st);
-    else if (cin == 32 && cout == 32) e = launch_wgrad_t<32, 32>(x, dy, dw, db, nx, ny, nz, st);
-    else if (cin == 32 && cout == 16) e = launch_wgrad_t<32, 16>(x, dy, dw, db, nx, ny, nz, st);
+    if (cin == 16 && cout == 32) e = launch_wgrad_tc_t<16, 32>(x, dy, dw, db, nx, ny, nz, st);
+    else if (cin == 32 && cout == 32) e = launch_wgrad_tc_t<32, 32>(x, dy, dw, db, nx, ny, nz, st);
+    else if (cin == 32 && cout == 16) e = launch_wgrad_tc_t<32, 16>(x, dy, dw, db, nx, ny, nz, st);
     else return MHD3D_ERR_ARG;
     return e == cudaSuccess ? MHD3D_OK : MHD3D_ERR_CUDA;
 }

@@ -14,6 +14,7 @@
 
 #include "../../include/mhd3d.h"
 #include "mhd3d_dev.cuh"
+#include "ring.cuh"
 #include "smem_attr.cuh"
 
 namespace mhd3d {
@@ -30,10 +31,17 @@ struct Handle {
     int cur = 0;               // ubuf[cur] holds the current state
     CUtensorMap map_u[2];      // TMA maps of the two U buffers
     CUtensorMap map_z;
+    CUtensorMap emap_u[2];     // the same for the tile rows of an ensemble (FP32 members)
+    CUtensorMap emap_z;
+    int ety = 0;               // tile rows emap_* were made for (0: none)
     double* z = nullptr;
     double* stage = nullptr;   // one Fortran (NX,NY,NZ) field
+    double* stage2 = nullptr;  // a second one: upload/download alternate between the two
+    cudaStream_t cst = nullptr;             // host<->device copies of upload/download
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr}, ev_kern[2] = {nullptr, nullptr};
     double* fout = nullptr;
     double* met = nullptr;     // all 1-D arrays, packed
+    float* metf = nullptr;     // FP32 copies for the fast-mode CFL screening, packed
     Control* ctl = nullptr;
     Accum* acc = nullptr;
     Metrics m{};
@@ -66,6 +74,8 @@ struct Handle {
     cudaStream_t own = nullptr;   // the handle's stream; st may be a caller's
     // asynchronous stepping: state at the last sync and steps enqueued since
     int nit_base = 0, cur_base = 0, pending = 0;
+    // poll limit of the stage kernels' first ring wait (tests lower it)
+    long long wait_first = WAIT_LIMIT;
     // per-stage event timing
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -838,6 +848,7 @@ StageArgs make_args(Handle* h)
     a.ntx = h->ntx;
     a.zlen = h->zlen;
     a.nchunks = h->nchunks;
+    a.wait_first = h->wait_first;
     return a;
 }
 
@@ -941,9 +952,16 @@ int destroy(Handle* h)
     cudaFree(h->ubuf[1]);
     cudaFree(h->z);
     cudaFree(h->stage);
+    cudaFree(h->stage2);
+    for (int i = 0; i < 2; ++i) {
+        if (h->ev_copy[i]) cudaEventDestroy(h->ev_copy[i]);
+        if (h->ev_kern[i]) cudaEventDestroy(h->ev_kern[i]);
+    }
+    if (h->cst) cudaStreamDestroy(h->cst);
     cudaFree(h->fout);
     cudaFree(h->hpart);
     cudaFree(h->met);
+    cudaFree(h->metf);
     cudaFree(h->bgd);
     cudaFree(h->bg32);
     cudaFree(h->pb);
@@ -1020,6 +1038,12 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
         CK(cudaMemset(h->pb, 0, sizeof(PlaneBg) * npz));
     }
     CK(cudaMalloc(&h->stage, sizeof(double) * (size_t)NX * NY * NZ));
+    CK(cudaMalloc(&h->stage2, sizeof(double) * (size_t)NX * NY * NZ));
+    CK(cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->ev_kern[i], cudaEventDisableTiming));
+    }
     CK(cudaMalloc(&h->ctl, sizeof(Control)));
     CK(cudaMalloc(&h->acc, sizeof(Accum)));
 
@@ -1161,6 +1185,36 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     h->m.rddy = h->met + offs[23];
     h->m.rddz = h->met + offs[24];
     h->m.fw2z = h->met + offs[25];
+    {
+        // FP32 screening copies: 1/DD and DD per axis, MIN(0.375*RE, 0.5*REPR*CV/RKAPA(K))
+        const size_t nf = 2 * ((size_t)NX + NY + NZ) + NZ;
+        std::vector<float> fm(nf);
+        size_t o = 0;
+        const double* dd[3] = {src[2], src[5], src[8]};
+        const int len[3] = {NX, NY, NZ};
+        size_t fo[7];
+        for (int d = 0; d < 3; ++d) {
+            fo[d] = o;
+            for (int i = 0; i < len[d]; ++i) fm[o + i] = (float)(1.0 / dd[d][i]);
+            o += len[d];
+        }
+        for (int d = 0; d < 3; ++d) {
+            fo[3 + d] = o;
+            for (int i = 0; i < len[d]; ++i) fm[o + i] = (float)dd[d][i];
+            o += len[d];
+        }
+        fo[6] = o;
+        for (int k = 0; k < NZ; ++k) fm[o + k] = (float)std::min(0.375 * p->re, hm[offs[25] + k]);
+        CK(cudaMalloc(&h->metf, sizeof(float) * nf));
+        CK(cudaMemcpy(h->metf, fm.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
+        h->m.rddx_f = h->metf + fo[0];
+        h->m.rddy_f = h->metf + fo[1];
+        h->m.rddz_f = h->metf + fo[2];
+        h->m.ddx_f = h->metf + fo[3];
+        h->m.ddy_f = h->metf + fo[4];
+        h->m.ddz_f = h->metf + fo[5];
+        h->m.wfz_f = h->metf + fo[6];
+    }
 
     // scalars (3dmhd.f:105-240 values; FLUXES/BCON per-call products)
     Scalars& s = h->s;
@@ -1176,6 +1230,9 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     s.tmp_13 = p->c13 * p->ore;
     s.tmp_m = p->obeta * p->orm * p->ocv;
     s.cw3 = 0.375 * p->re;
+    s.ogamma_f = (float)(1.0 / p->gamma);
+    s.gamma_f = (float)p->gamma;
+    s.obeta_f = (float)p->obeta;
     {
         Scalars32& f = h->s32;
         f.grav = (float)p->grav; f.ore = (float)p->ore; f.c13 = (float)p->c13; f.c43 = (float)p->c43;
@@ -1312,6 +1369,10 @@ int set_background(Handle* h)
     return MHD3D_OK;
 }
 
+// Upload and download move one field at a time through two staging fields:
+// the copy of field i (on the copy stream) overlaps the unpack or pack of
+// field i-1 (on the handle's stream); events order each staging field's
+// copy, kernel and reuse two fields later.
 int upload(Handle* h, const double* const f[8])
 {
     CK(cudaSetDevice(h->dev));
@@ -1319,21 +1380,30 @@ int upload(Handle* h, const double* const f[8])
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
     for (int i = 0; i < h->nf; ++i)
         if (!f[i]) return MHD3D_ERR_ARG;
+    // the staging fields are free once the handle's stream has drained
+    CK(cudaEventRecord(h->ev_kern[1], h->st));
+    CK(cudaStreamWaitEvent(h->cst, h->ev_kern[1], 0));
     for (int fi = 0; fi < h->nf; ++fi) {
-        CK(cudaMemcpyAsync(h->stage, f[fi], sizeof(double) * nfort, cudaMemcpyDefault, h->st));
+        const int b = fi & 1;
+        double* const stg = b ? h->stage2 : h->stage;
+        if (fi >= 2) CK(cudaStreamWaitEvent(h->cst, h->ev_kern[b], 0));   // field fi-2 unpacked
+        CK(cudaMemcpyAsync(stg, f[fi], sizeof(double) * nfort, cudaMemcpyDefault, h->cst));
+        CK(cudaEventRecord(h->ev_copy[b], h->cst));
+        CK(cudaStreamWaitEvent(h->st, h->ev_copy[b], 0));
         if (h->f32) {
             const int bi = bg_index(fi);
             double* bg = bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr;
-            if (bg) k_hmean<<<npz + 2, 256, 0, h->st>>>(h->stage, bg, npx, npy);
+            if (bg) k_hmean<<<npz + 2, 256, 0, h->st>>>(stg, bg, npx, npy);
             float* u0 = reinterpret_cast<float*>(h->ubuf[0]) + (size_t)fi * h->uf;
             float* u1 = reinterpret_cast<float*>(h->ubuf[1]) + (size_t)fi * h->uf;
-            k_unpack32<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, bg, u0, u1, npx, npy, npz, h->upitch, h->uz);
+            k_unpack32<<<grid_for(nfort), 256, 0, h->st>>>(stg, bg, u0, u1, npx, npy, npz, h->upitch, h->uz);
         } else {
-            k_unpack<<<grid_for(nfort), 256, 0, h->st>>>(h->stage, h->ubuf[0] + (size_t)fi * h->uf,
+            k_unpack<<<grid_for(nfort), 256, 0, h->st>>>(stg, h->ubuf[0] + (size_t)fi * h->uf,
                                                          h->ubuf[1] + (size_t)fi * h->uf, npx, npy, npz, h->upitch,
                                                          h->uz);
         }
         CK(cudaGetLastError());
+        CK(cudaEventRecord(h->ev_kern[b], h->st));
     }
     CK(cudaStreamSynchronize(h->st));
     if (h->f32) {
@@ -1351,20 +1421,29 @@ int download(Handle* h, double* const f[8])
     CK(cudaSetDevice(h->dev));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nfort = (size_t)(npx + 2) * (npy + 2) * (npz + 2);
+    int n = 0;
     for (int fi = 0; fi < h->nf; ++fi) {
         if (!f[fi]) continue;
+        const int b = n & 1;
+        double* const stg = b ? h->stage2 : h->stage;
+        if (n >= 2) CK(cudaStreamWaitEvent(h->st, h->ev_copy[b], 0));   // the copy of two fields ago done
         if (h->f32) {
             const int bi = bg_index(fi);
             k_pack32<<<grid_for(nfort), 256, 0, h->st>>>(
                 reinterpret_cast<const float*>(h->ubuf[h->cur]) + (size_t)fi * h->uf,
-                bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr, h->stage, npx, npy, npz, h->upitch, h->uz);
+                bi >= 0 ? h->bgd + (size_t)bi * (npz + 2) : nullptr, stg, npx, npy, npz, h->upitch, h->uz);
         } else {
-            k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->uf, h->stage, npx, npy,
+            k_pack<<<grid_for(nfort), 256, 0, h->st>>>(h->ubuf[h->cur] + (size_t)fi * h->uf, stg, npx, npy,
                                                        npz, h->upitch, h->uz);
         }
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(f[fi], h->stage, sizeof(double) * nfort, cudaMemcpyDefault, h->st));
+        CK(cudaEventRecord(h->ev_kern[b], h->st));
+        CK(cudaStreamWaitEvent(h->cst, h->ev_kern[b], 0));
+        CK(cudaMemcpyAsync(f[fi], stg, sizeof(double) * nfort, cudaMemcpyDefault, h->cst));
+        CK(cudaEventRecord(h->ev_copy[b], h->cst));
+        ++n;
     }
+    CK(cudaStreamSynchronize(h->cst));
     CK(cudaStreamSynchronize(h->st));
     return MHD3D_OK;
 }
@@ -1625,6 +1704,7 @@ struct Ensemble {
     cudaStream_t st = nullptr;
     int dev = -1, lmag = 0, lrot = 0, sms = 148;
     int ctas_per_sm = 4;                    // persistent CTAs per SM
+    int ty = TY32;                          // tile rows (TX x ty columns a tile)
     StageArgs32* dargs[2] = {nullptr, nullptr};
     int* dorder = nullptr;                  // members by decreasing work
     int* dbase = nullptr;                   // first item of each member in that order (+ total)
@@ -1662,7 +1742,7 @@ int ens_layout(Ensemble* e)
     std::vector<long> items(n);
     for (int i = 0; i < n; ++i) {
         Handle* h = e->mem[i];
-        items[i] = (long)h->ntx * ((h->p.npy + TY32 - 1) / TY32) * h->nchunks;
+        items[i] = (long)h->ntx * ((h->p.npy + e->ty - 1) / e->ty) * h->nchunks;
     }
     e->order.resize(n);
     for (int i = 0; i < n; ++i) e->order[i] = i;
@@ -1680,6 +1760,8 @@ int ens_layout(Ensemble* e)
         }
     return MHD3D_OK;
 }
+
+int ens_set_tile(Ensemble* e, int ty);
 
 int ens_create(int n, const mhd3d_params* ps, const double* const* grids, Ensemble** out)
 {
@@ -1714,8 +1796,41 @@ int ens_create(int n, const mhd3d_params* ps, const double* const* grids, Ensemb
         fin[i] = FinArgs{h->ctl, h->acc, h->s.sf, h->s.dtmin, h->w4key, h->p.lmag, 0};
     }
     CK(cudaMemcpy(e->dfin, fin.data(), sizeof(FinArgs) * n, cudaMemcpyHostToDevice));
-    for (int stg = 1; stg <= 3; ++stg)   // kernel attributes are set outside any graph capture
-        CK(f32::launch_stage_multi(stg, e->lmag, e->lrot, nullptr, nullptr, nullptr, 0, nullptr, 0, e->st));
+    for (int ty : {2, 4, 8})   // kernel attributes are set outside any graph capture
+        for (int stg = 1; stg <= 3; ++stg)
+            CK(f32::launch_stage_multi(stg, e->lmag, e->lrot, ty, nullptr, nullptr, nullptr, 0, nullptr, 0, e->st));
+    if (int st = ens_set_tile(e, TY32)) return st;
+    return ens_layout(e);
+}
+
+// tile rows every member can take: boxes of ty+2 U rows and ty Z rows must
+// fit the padded arrays
+bool ens_tile_fits(const Ensemble* e, int ty)
+{
+    if (!f32::multi_tile_rows_ok(ty)) return false;
+    for (const Handle* h : e->mem)
+        if (ty + 2 > h->urows || ty > h->zrows) return false;
+    return true;
+}
+
+// set the ensemble's tile rows: TMA maps of every member for that box height
+// (emap_*, used by the ensemble's argument tables only) and the work table
+int ens_set_tile(Ensemble* e, int ty)
+{
+    if (!ens_tile_fits(e, ty)) return MHD3D_ERR_ARG;
+    for (Handle* h : e->mem) {
+        const int NZ = h->p.npz + 2;
+        const cuuint64_t du[4] = {(cuuint64_t)h->upitch, (cuuint64_t)h->urows, (cuuint64_t)NZ, (cuuint64_t)h->nf};
+        const cuuint32_t bu[4] = {(cuuint32_t)BW32, (cuuint32_t)(ty + 2), 1, (cuuint32_t)h->nf};
+        for (int b = 0; b < 2; ++b)
+            if (int st = make_map(&h->emap_u[b], h->ubuf[b], du, bu, true)) return st;
+        const cuuint64_t dz[4] = {(cuuint64_t)h->zpitch, (cuuint64_t)h->zrows, (cuuint64_t)h->p.npz,
+                                  (cuuint64_t)h->nf};
+        const cuuint32_t bz[4] = {TX, (cuuint32_t)ty, 1, (cuuint32_t)h->nf};
+        if (int st = make_map(&h->emap_z, h->z, dz, bz, true)) return st;
+        h->ety = ty;
+    }
+    e->ty = ty;
     return ens_layout(e);
 }
 
@@ -1743,7 +1858,7 @@ int ens_capture(Ensemble* e, int q)
     const int n = (int)e->mem.size();
     cudaError_t err = cudaMemsetAsync(e->dcount, 0, sizeof(unsigned) * 4, e->st);
     for (int stg = 1; stg <= 3 && err == cudaSuccess; ++stg)
-        err = f32::launch_stage_multi(stg, e->lmag, e->lrot, e->dargs[(stg == 2) ? (q ^ 1) : q], e->dorder,
+        err = f32::launch_stage_multi(stg, e->lmag, e->lrot, e->ty, e->dargs[(stg == 2) ? (q ^ 1) : q], e->dorder,
                                       e->dbase, n, e->dcount + (stg - 1), nb, e->st);
     if (err == cudaSuccess) {
         k_finalize_multi<<<(n + 127) / 128, 128, 0, e->st>>>(e->dfin, n);
@@ -1783,7 +1898,8 @@ int ens_step(Ensemble* e, int nsteps)
         for (int p = 0; p < 2; ++p) {
             StageArgs32 a = make_args32(h);
             const int in = cur ^ p;
-            a.map_u = h->map_u[in];
+            a.map_u = h->emap_u[in];   // the ensemble's tile rows
+            a.map_z = h->emap_z;
             a.u_in = reinterpret_cast<const float*>(h->ubuf[in]);
             a.u_out = reinterpret_cast<float*>(h->ubuf[in ^ 1]);
             tab[p][i] = a;
@@ -1873,32 +1989,43 @@ int ens_tune(Ensemble* e, int steps, int32_t* zlen_out, int32_t* ctas_out, doubl
         CK(cudaStreamSynchronize(e->st));
         return MHD3D_OK;
     };
+    // search: tile rows (32 x 2, 32 x 4, 32 x 8 columns a tile, separate
+    // kernel instances) x z chunk length x persistent CTAs per SM (8, 12 or 16
+    // warps an SM where the tile allows)
     const int zc[] = {4, 6, 8, 12, 16, 24, 32, 48, 64};
-    const int cc[] = {2, 3, 4};
-    int best_z = 0, best_c = e->ctas_per_sm;
+    struct TileChoice {
+        int ty, nc, cc[3];
+    };
+    const TileChoice tcs[] = {{2, 3, {4, 6, 8}}, {4, 3, {2, 3, 4}}, {8, 2, {1, 2, 0}}};
+    int best_z = 0, best_c = e->ctas_per_sm, best_t = e->ty;
     double best = 1e300;
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     int st = MHD3D_OK;
-    for (int zi = 0; zi < (int)(sizeof(zc) / sizeof(zc[0])) && !st; ++zi) {
-        if (zc[zi] > maxnpz) break;
-        for (int ci = 0; ci < 3 && !st; ++ci) {
-            e->ctas_per_sm = cc[ci];
-            if ((st = ens_set_zlen(e, zc[zi]))) break;
-            if ((st = ens_step(e, 1))) break;   // warm-up, builds the graphs
-            cudaEventRecord(t0, e->st);
-            if ((st = ens_step(e, steps))) break;
-            cudaEventRecord(t1, e->st);
-            if (cudaEventSynchronize(t1) != cudaSuccess) { st = MHD3D_ERR_CUDA; break; }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, t0, t1);
-            if ((st = restore())) break;
-            const double per = ms / std::max(steps, 1);
-            if (per < best) {
-                best = per;
-                best_z = zc[zi];
-                best_c = cc[ci];
+    for (const TileChoice& tc : tcs) {
+        if (st || !ens_tile_fits(e, tc.ty)) continue;
+        if ((st = ens_set_tile(e, tc.ty))) break;
+        for (int zi = 0; zi < (int)(sizeof(zc) / sizeof(zc[0])) && !st; ++zi) {
+            if (zc[zi] > maxnpz) break;
+            for (int ci = 0; ci < tc.nc && !st; ++ci) {
+                e->ctas_per_sm = tc.cc[ci];
+                if ((st = ens_set_zlen(e, zc[zi]))) break;
+                if ((st = ens_step(e, 1))) break;   // warm-up, builds the graphs
+                cudaEventRecord(t0, e->st);
+                if ((st = ens_step(e, steps))) break;
+                cudaEventRecord(t1, e->st);
+                if (cudaEventSynchronize(t1) != cudaSuccess) { st = MHD3D_ERR_CUDA; break; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, t0, t1);
+                if ((st = restore())) break;
+                const double per = ms / std::max(steps, 1);
+                if (per < best) {
+                    best = per;
+                    best_z = zc[zi];
+                    best_c = tc.cc[ci];
+                    best_t = tc.ty;
+                }
             }
         }
     }
@@ -1909,6 +2036,7 @@ int ens_tune(Ensemble* e, int steps, int32_t* zlen_out, int32_t* ctas_out, doubl
     if (st) return st;
     if (st2) return st2;
     e->ctas_per_sm = best_c;
+    if (int s3 = ens_set_tile(e, best_t)) return s3;
     if (int s3 = ens_set_zlen(e, best_z)) return s3;
     if (zlen_out) *zlen_out = best_z;
     if (ctas_out) *ctas_out = best_c;
@@ -1990,6 +2118,15 @@ int mhd3d_set_stream(void* handle, void* stream)
     CK(cudaSetDevice(h->dev));
     CK(cudaStreamSynchronize(h->st));
     h->st = stream ? static_cast<cudaStream_t>(stream) : h->own;
+    return MHD3D_OK;
+}
+
+int mhd3d_set_wait_limit(void* handle, int64_t polls)
+{
+    if (!handle || polls < 0) return MHD3D_ERR_ARG;
+    Handle* h = static_cast<Handle*>(handle);
+    if (h->f32) return MHD3D_ERR_ARG;   // the FP64 stage kernels only
+    h->wait_first = polls ? (long long)std::min<int64_t>(polls, WAIT_LIMIT) : 0;
     return MHD3D_OK;
 }
 
@@ -2227,6 +2364,25 @@ int mhd3d_ensemble_set_stream(void* ens, void* stream)
     if (!e->own_st) e->own_st = e->st;
     e->st = stream ? static_cast<cudaStream_t>(stream) : e->own_st;
     for (Handle* h : e->mem) h->st = e->st;
+    return MHD3D_OK;
+}
+
+int mhd3d_ensemble_set_tile(void* ens, int32_t tile_y)
+{
+    if (!ens) return MHD3D_ERR_ARG;
+    Ensemble* e = static_cast<Ensemble*>(ens);
+    CK(cudaSetDevice(e->dev));
+    if (int st = ens_sync(e, nullptr, nullptr, nullptr, nullptr))
+        if (st == MHD3D_ERR_CUDA) return st;
+    return ens_set_tile(e, tile_y);
+}
+
+int mhd3d_ensemble_tile(void* ens, int32_t* tile_x, int32_t* tile_y)
+{
+    if (!ens) return MHD3D_ERR_ARG;
+    const Ensemble* e = static_cast<const Ensemble*>(ens);
+    if (tile_x) *tile_x = TX;
+    if (tile_y) *tile_y = e->ty;
     return MHD3D_OK;
 }
 

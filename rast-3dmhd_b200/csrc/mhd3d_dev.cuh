@@ -59,6 +59,7 @@ struct Scalars {
     double top_dz;     // DZ at the top wall
     double bot_flux;   // C23*DZ*THETA/RKAPA at the bottom wall (IZC=1, 2925-2941)
     double dtmin, timi;
+    float ogamma_f, gamma_f, obeta_f;   // 1/GAMMA, GAMMA, OBETA rounded to FP32 (fast-mode CFL screening)
     int npx, npy, npz, pitch;
     int lmag, lrot, izcon, itcon, ibcon, plume;
 };
@@ -93,6 +94,9 @@ struct Metrics {
     const double *fax, *fbx, *fcx, *fay, *fby, *fcy, *faz, *fbz, *fcz;
     // fast-mode CFL: 1/DDX, 1/DDY, 1/DDZ and 0.5*REPR*CV/RKAPA(K)
     const double *rddx, *rddy, *rddz, *fw2z;
+    // the same rounded to FP32 for the CFL screening: 1/DD and DD per axis,
+    // MIN(0.375*RE, 0.5*REPR*CV/RKAPA(K)) per plane
+    const float *rddx_f, *rddy_f, *rddz_f, *ddx_f, *ddy_f, *ddz_f, *wfz_f;
 };
 
 struct StageArgs {
@@ -112,6 +116,7 @@ struct StageArgs {
     int ntx;                // tiles along x
     int zlen;               // planes per z chunk
     int nchunks;
+    long long wait_first;   // poll limit of a CTA's first ring wait (WAIT_LIMIT; lowered only by tests)
 };
 
 // ---- FP32 form ----------------------------------------------------------
@@ -222,10 +227,13 @@ namespace f32 {
 size_t stage_smem_bytes(int lmag);
 cudaError_t launch_stage(int stage, const StageArgs32& a, cudaStream_t st);
 cudaError_t launch_cfl(const StageArgs32& a, cudaStream_t st);
-// persistent multi-grid form (ensembles): args, order, item_base in device memory;
-// nblocks == 0 only prepares the kernel attributes (before a graph capture)
-cudaError_t launch_stage_multi(int stage, int lmag, int lrot, const StageArgs32* args, const int* order,
+// persistent multi-grid form (ensembles) with tile rows ty (2, 4 or 8): args,
+// order, item_base in device memory; nblocks == 0 only prepares the kernel
+// attributes (before a graph capture)
+cudaError_t launch_stage_multi(int stage, int lmag, int lrot, int ty, const StageArgs32* args, const int* order,
                                const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st);
+bool multi_tile_rows_ok(int ty);
+size_t multi_smem_bytes(int lmag, int ty);
 }
 
 }  // namespace mhd3d

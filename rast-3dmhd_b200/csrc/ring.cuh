@@ -39,9 +39,9 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned pari
     return ok != 0;
 }
 // bounded wait for the phase with the given parity; false when it gave up
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long limit = WAIT_LIMIT)
 {
-    for (long it = 0; it < WAIT_LIMIT; ++it) {
+    for (long it = 0; it < limit; ++it) {
         if (mbar_test(bar, parity)) return true;
         if (it > 32) __nanosleep(128);
     }

@@ -40,15 +40,18 @@ constexpr int NRI = 3;
 
 constexpr size_t al128(size_t b) { return (b + 127) / 128 * 128; }
 
-template <bool MAG>
+// shared-memory layout of a CTA with TYV tile rows (TX x TYV threads)
+template <bool MAG, int TYV = TY32>
 struct Lay32 {
     static constexpr int NF = MAG ? 8 : 5;
-    static constexpr size_t RAW_SLOT_B = al128((size_t)NF * BSLOT32 * 4);
+    static constexpr int NTV = TX * TYV;                  // threads
+    static constexpr int BSV = BW32 * (TYV + 2);          // floats of one field in one plane box
+    static constexpr size_t RAW_SLOT_B = al128((size_t)NF * BSV * 4);
     static constexpr size_t RI_OFF_B = NRAW * RAW_SLOT_B;
-    static constexpr size_t Z_OFF_B = al128(RI_OFF_B + (size_t)NRI * BSLOT32 * 4);
-    static constexpr size_t BAR_OFF_B = al128(Z_OFF_B + (size_t)NF * TY32 * TX * 4);
+    static constexpr size_t Z_OFF_B = al128(RI_OFF_B + (size_t)NRI * BSV * 4);
+    static constexpr size_t BAR_OFF_B = al128(Z_OFF_B + (size_t)NF * TYV * TX * 4);
     static constexpr size_t RED_OFF_B = BAR_OFF_B + 8 * 8;
-    static constexpr size_t FLAG_OFF_B = RED_OFF_B + (size_t)(NT32 / 32) * 3 * 8;
+    static constexpr size_t FLAG_OFF_B = RED_OFF_B + (size_t)(NTV / 32) * 3 * 8;
     static constexpr size_t BYTES = FLAG_OFF_B + 16 + 128;   // + alignment slack
 };
 
@@ -56,25 +59,25 @@ enum Q32 { P_RU = 0, P_RV, P_RW, P_RO, P_TT, P_RI, P_UU, P_VV, P_WW, P_PP, P_BX,
 
 // quantity QQ at offset off of a plane slot whose background is (rob, ttb):
 // stored fields, 1/RO, velocities, and the pressure perturbation
-template <int QQ>
+template <int QQ, int BS = BSLOT32>
 __device__ __forceinline__ float qf(const float* __restrict__ raw, const float* __restrict__ ri, int off, float rob,
                                     float ttb)
 {
-    if constexpr (QQ == P_RU) return raw[F_RU * BSLOT32 + off];
-    else if constexpr (QQ == P_RV) return raw[F_RV * BSLOT32 + off];
-    else if constexpr (QQ == P_RW) return raw[F_RW * BSLOT32 + off];
-    else if constexpr (QQ == P_RO) return raw[F_RO * BSLOT32 + off];
-    else if constexpr (QQ == P_TT) return raw[F_TT * BSLOT32 + off];
-    else if constexpr (QQ == P_BX) return raw[F_BX * BSLOT32 + off];
-    else if constexpr (QQ == P_BY) return raw[F_BY * BSLOT32 + off];
-    else if constexpr (QQ == P_BZ) return raw[F_BZ * BSLOT32 + off];
+    if constexpr (QQ == P_RU) return raw[F_RU * BS + off];
+    else if constexpr (QQ == P_RV) return raw[F_RV * BS + off];
+    else if constexpr (QQ == P_RW) return raw[F_RW * BS + off];
+    else if constexpr (QQ == P_RO) return raw[F_RO * BS + off];
+    else if constexpr (QQ == P_TT) return raw[F_TT * BS + off];
+    else if constexpr (QQ == P_BX) return raw[F_BX * BS + off];
+    else if constexpr (QQ == P_BY) return raw[F_BY * BS + off];
+    else if constexpr (QQ == P_BZ) return raw[F_BZ * BS + off];
     else if constexpr (QQ == P_RI) return ri[off];
-    else if constexpr (QQ == P_UU) return raw[F_RU * BSLOT32 + off] * ri[off];
-    else if constexpr (QQ == P_VV) return raw[F_RV * BSLOT32 + off] * ri[off];
-    else if constexpr (QQ == P_WW) return raw[F_RW * BSLOT32 + off] * ri[off];
+    else if constexpr (QQ == P_UU) return raw[F_RU * BS + off] * ri[off];
+    else if constexpr (QQ == P_VV) return raw[F_RV * BS + off] * ri[off];
+    else if constexpr (QQ == P_WW) return raw[F_RW * BS + off] * ri[off];
     else {
-        const float t = raw[F_TT * BSLOT32 + off];
-        return rob * t + raw[F_RO * BSLOT32 + off] * (ttb + t);
+        const float t = raw[F_TT * BS + off];
+        return rob * t + raw[F_RO * BS + off] * (ttb + t);
     }
 }
 
@@ -149,11 +152,12 @@ __device__ __forceinline__ void cfl32_commit(Accum* acc, unsigned long long* red
 // `a`, on the CTA's shared memory `sb` (128-byte aligned).  On return every
 // TMA copy the item issued has landed and its mbarriers are invalidated, so
 // a persistent CTA can take the next item.
-template <bool MAG, bool ROT, int STAGE>
+template <bool MAG, bool ROT, int STAGE, int TYV = TY32>
 __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int tile, const int chunk,
                                              unsigned char* const sb)
 {
-    using L = Lay32<MAG>;
+    using L = Lay32<MAG, TYV>;
+    constexpr int TYL = TYV, NTL = L::NTV, BSL = L::BSV;
     constexpr int NF = L::NF;
     float* const sraw = reinterpret_cast<float*>(sb);
     float* const sri = reinterpret_cast<float*>(sb + L::RI_OFF_B);
@@ -168,7 +172,7 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
     const int npx = s.npx, npy = s.npy, npz = s.npz;
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY32;
+    const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TYL;
     const int k0 = chunk * a.zlen;
     const int k1 = (chunk == a.nchunks - 1) ? npz : k0 + a.zlen;
     const int gi = x0 + tx, gj = y0 + ty;
@@ -188,8 +192,8 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
     const float rddxy = fmaxf(cxc.rdd, cyc.rdd);
     const float ddxy = fminf(cxc.dd, cyc.dd);
 
-    const unsigned raw_bytes = (unsigned)(NF * BSLOT32 * 4);
-    const unsigned z_bytes = (unsigned)(NF * TY32 * TX * 4);
+    const unsigned raw_bytes = (unsigned)(NF * BSL * 4);
+    const unsigned z_bytes = (unsigned)(NF * TYL * TX * 4);
     const size_t ucol = (size_t)(gj + 1) * a.upitch + (gi + 1);
     const size_t zcol = (size_t)gj * a.zpitch + gi;
     const HaloCols hc = halo_cols(npx, npy, a.upitch, gi, gj);
@@ -228,10 +232,10 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
                                               (size_t)((kp + 1) & 3) * L::RAW_SLOT_B);
     };
     auto derive_ri = [&](int kp) {
-        const float* r = slot(kp) + F_RO * BSLOT32;
-        float* d = sri + (size_t)((kp + 1) % 3) * BSLOT32;
+        const float* r = slot(kp) + F_RO * BSL;
+        float* d = sri + (size_t)((kp + 1) % 3) * BSL;
         const float rb = a.rob[kp + 1];
-        for (int p = tid; p < BSLOT32; p += NT32) d[p] = __frcp_rn(rb + r[p]);
+        for (int p = tid; p < BSL; p += NTL) d[p] = __frcp_rn(rb + r[p]);
     };
 
     if (tid == 0)
@@ -267,15 +271,15 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
             const float* Rm = slot(k - 1);
             const float* Rc = slot(k);
             const float* Rp = slot(k + 1);
-            const float* Im = sri + (size_t)((k + 0) % 3) * BSLOT32;
-            const float* Ic = sri + (size_t)((k + 1) % 3) * BSLOT32;
-            const float* Ip = sri + (size_t)((k + 2) % 3) * BSLOT32;
+            const float* Im = sri + (size_t)((k + 0) % 3) * BSL;
+            const float* Ic = sri + (size_t)((k + 1) % 3) * BSL;
+            const float* Ip = sri + (size_t)((k + 2) % 3) * BSL;
             const PlaneBg& pb = a.pb[k];
             const float robm = pb.robm, robc = pb.robc, robp = pb.robp;
             const float ttbm = pb.ttbm, ttbc = pb.ttbc, ttbp = pb.ttbp;
-#define C_(q, dx, dy) qf<q>(Rc, Ic, (ly + (dy)) * BW32 + (lx + (dx)), robc, ttbc)
-#define M_(q, dx, dy) qf<q>(Rm, Im, (ly + (dy)) * BW32 + (lx + (dx)), robm, ttbm)
-#define P_(q, dx, dy) qf<q>(Rp, Ip, (ly + (dy)) * BW32 + (lx + (dx)), robp, ttbp)
+#define C_(q, dx, dy) qf<q, BSL>(Rc, Ic, (ly + (dy)) * BW32 + (lx + (dx)), robc, ttbc)
+#define M_(q, dx, dy) qf<q, BSL>(Rm, Im, (ly + (dy)) * BW32 + (lx + (dx)), robm, ttbm)
+#define P_(q, dx, dy) qf<q, BSL>(Rp, Ip, (ly + (dy)) * BW32 + (lx + (dx)), robp, ttbp)
             const bool top = (k == 0), bot = (k == npz - 1);
             const float az = pb.az, bzq = pb.bzq, czq = pb.czq, rka = pb.rka, dka = pb.dka;
             // own column two and three planes inside the wall (one-sided stencils)
@@ -466,15 +470,15 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
                 } else {
                     zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
                     const float* zt_ = sz + ty * TX + tx;
-                    zu = zt_[F_RU * TY32 * TX];
-                    zv = zt_[F_RV * TY32 * TX];
-                    zw = zt_[F_RW * TY32 * TX];
-                    zt = zt_[F_TT * TY32 * TX];
-                    zr = zt_[F_RO * TY32 * TX];
+                    zu = zt_[F_RU * TYL * TX];
+                    zv = zt_[F_RV * TYL * TX];
+                    zw = zt_[F_RW * TYL * TX];
+                    zt = zt_[F_TT * TYL * TX];
+                    zr = zt_[F_RO * TYL * TX];
                     if (MAG) {
-                        zbx = zt_[F_BX * TY32 * TX];
-                        zby = zt_[F_BY * TY32 * TX];
-                        zbz = zt_[F_BZ * TY32 * TX];
+                        zbx = zt_[F_BX * TYL * TX];
+                        zby = zt_[F_BY * TYL * TX];
+                        zbz = zt_[F_BZ * TYL * TX];
                     }
                 }
                 const float nu = zu + cu * fu, nv = zv + cu * fv, nw = zw + cu * fw;
@@ -618,8 +622,14 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32) k_stage32(const __grid_con
 #ifndef MHD3D_MINB32M
 #define MHD3D_MINB32M 4   // the persistent form carries its loop state as well: 128 registers, no spills
 #endif
-template <bool MAG, bool ROT, int STAGE>
-__global__ void __launch_bounds__(NT32, MHD3D_MINB32M) k_stage32_multi(const StageArgs32* __restrict__ args,
+// CTAs per SM the register budget of each tile height is sized for (128
+// registers a thread in each case)
+template <int TYV>
+struct MultiMinB {
+    static constexpr int v = TYV == 2 ? 8 : TYV == 4 ? MHD3D_MINB32M : 2;
+};
+template <bool MAG, bool ROT, int STAGE, int TYV>
+__global__ void __launch_bounds__(TX * TYV, MultiMinB<TYV>::v) k_stage32_multi(const StageArgs32* __restrict__ args,
                                                                       const int* __restrict__ order,
                                                                       const int* __restrict__ item_base, int nmem,
                                                                       unsigned* counter)
@@ -641,9 +651,9 @@ __global__ void __launch_bounds__(NT32, MHD3D_MINB32M) k_stage32_multi(const Sta
             else hi = mid - 1;
         }
         const StageArgs32& a = args[order[lo]];
-        const int ntiles = a.ntx * ((a.s.npy + TY32 - 1) / TY32);
+        const int ntiles = a.ntx * ((a.s.npy + TYV - 1) / TYV);
         const int local = it - item_base[lo];
-        stage32_item<MAG, ROT, STAGE>(a, local % ntiles, local / ntiles, sb);
+        stage32_item<MAG, ROT, STAGE, TYV>(a, local % ntiles, local / ntiles, sb);
         __syncthreads();
     }
 }
@@ -734,20 +744,20 @@ cudaError_t launch_stage(int stage, const StageArgs32& a, cudaStream_t st)
 
 size_t stage_smem_bytes(int lmag) { return lmag ? Lay32<true>::BYTES : Lay32<false>::BYTES; }
 
-template <bool MAG, bool ROT>
+template <bool MAG, bool ROT, int TYV>
 static cudaError_t launch_multi_t(int stage, const StageArgs32* args, const int* order, const int* item_base,
                                   int nmem, unsigned* counter, int nblocks, cudaStream_t st)
 {
-    const size_t smem = Lay32<MAG>::BYTES;
+    const size_t smem = Lay32<MAG, TYV>::BYTES;
     switch (stage) {
 #define L_(S)                                                                                              \
     case S: {                                                                                              \
         static std::atomic<unsigned long long> attr_set{0};                                                \
-        cudaError_t ae = smem_attr_once(attr_set, reinterpret_cast<const void*>(k_stage32_multi<MAG, ROT, S>), \
+        cudaError_t ae = smem_attr_once(attr_set, reinterpret_cast<const void*>(k_stage32_multi<MAG, ROT, S, TYV>), \
                                         smem);                                                             \
         if (ae != cudaSuccess) return ae;                                                                  \
         if (nblocks > 0)                                                                                   \
-            k_stage32_multi<MAG, ROT, S><<<nblocks, NT32, smem, st>>>(args, order, item_base, nmem, counter); \
+            k_stage32_multi<MAG, ROT, S, TYV><<<nblocks, TX * TYV, smem, st>>>(args, order, item_base, nmem, counter); \
         break;                                                                                             \
     }
         L_(1) L_(2) L_(3)
@@ -758,14 +768,35 @@ static cudaError_t launch_multi_t(int stage, const StageArgs32* args, const int*
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage_multi(int stage, int lmag, int lrot, const StageArgs32* args, const int* order,
-                               const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st)
+template <int TYV>
+static cudaError_t launch_multi_ty(int stage, int lmag, int lrot, const StageArgs32* args, const int* order,
+                                   const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st)
 {
     if (lmag)
-        return lrot ? launch_multi_t<true, true>(stage, args, order, item_base, nmem, counter, nblocks, st)
-                    : launch_multi_t<true, false>(stage, args, order, item_base, nmem, counter, nblocks, st);
-    return lrot ? launch_multi_t<false, true>(stage, args, order, item_base, nmem, counter, nblocks, st)
-                : launch_multi_t<false, false>(stage, args, order, item_base, nmem, counter, nblocks, st);
+        return lrot ? launch_multi_t<true, true, TYV>(stage, args, order, item_base, nmem, counter, nblocks, st)
+                    : launch_multi_t<true, false, TYV>(stage, args, order, item_base, nmem, counter, nblocks, st);
+    return lrot ? launch_multi_t<false, true, TYV>(stage, args, order, item_base, nmem, counter, nblocks, st)
+                : launch_multi_t<false, false, TYV>(stage, args, order, item_base, nmem, counter, nblocks, st);
+}
+
+bool multi_tile_rows_ok(int ty) { return ty == 2 || ty == 4 || ty == 8; }
+
+size_t multi_smem_bytes(int lmag, int ty)
+{
+    if (ty == 2) return lmag ? Lay32<true, 2>::BYTES : Lay32<false, 2>::BYTES;
+    if (ty == 8) return lmag ? Lay32<true, 8>::BYTES : Lay32<false, 8>::BYTES;
+    return lmag ? Lay32<true, 4>::BYTES : Lay32<false, 4>::BYTES;
+}
+
+cudaError_t launch_stage_multi(int stage, int lmag, int lrot, int ty, const StageArgs32* args, const int* order,
+                               const int* item_base, int nmem, unsigned* counter, int nblocks, cudaStream_t st)
+{
+    switch (ty) {
+    case 2: return launch_multi_ty<2>(stage, lmag, lrot, args, order, item_base, nmem, counter, nblocks, st);
+    case 4: return launch_multi_ty<4>(stage, lmag, lrot, args, order, item_base, nmem, counter, nblocks, st);
+    case 8: return launch_multi_ty<8>(stage, lmag, lrot, args, order, item_base, nmem, counter, nblocks, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_cfl(const StageArgs32& a, cudaStream_t st)

@@ -54,7 +54,7 @@ struct Lay {
     static constexpr int Z_OFF = ((RI_OFF + NRI * BSLOT) * 8 + 127) / 128 * 128 / 8;
     static constexpr int BAR_OFF = Z_OFF + ZT;           // 5 mbarriers (8 B each)
     static constexpr int RED_OFF = BAR_OFF + 8;          // CFL block reduction
-    static constexpr int FLAG_OFF = RED_OFF + (NT / 32) * 6;
+    static constexpr int FLAG_OFF = RED_OFF + (NT / 32) * 8;   // 3 keys + a 40-byte screening record per warp
     static constexpr int TOTAL = FLAG_OFF + 2;
     static constexpr size_t BYTES = (size_t)TOTAL * 8 + 128;   // + alignment slack
 };
@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         r[1] = 0ull;
         r[2] = 0ull;
     }
+    if (STAGE == 3) cfl_screen_init(red, a.acc, a.s, MAG);
     __syncthreads();
     if (*sflag < 0) return;
 
@@ -237,7 +238,11 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
 
     if (tid == 0)
         for (int kp = k0 - 1; kp <= k0 - 2 + NRAW && kp <= k1; ++kp) issue_plane(kp);
-    bool ok = mbar_wait(&bars[(k0 + 0) % NRAW], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) % NRAW], parity_of(k0));
+    // the first wait's limit is a launch argument (a test lowers it to make
+    // the wait give up); every other wait, the drain's included, is bounded
+    // by WAIT_LIMIT
+    bool ok = mbar_wait(&bars[(k0 + 0) % NRAW], parity_of(k0 - 1), (long)a.wait_first) &&
+              mbar_wait(&bars[(k0 + 1) % NRAW], parity_of(k0));
     if (ok) {
         derive_ri(k0 - 1);
         derive_ri(k0);
@@ -698,7 +703,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                 }
                 // ---- BCON (3dmhdsub.f:2751-2955) and the CFL parts of the next step
                 if (!top && !bot) {
-                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, nu, nv, nw, nr, nt, nbx, nby, nbz);
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, k, nu, nv, nw, nr, nt, nbx, nby, nbz);
                 }
                 if (k == 2 && k0 == 0) {
                     // top wall: new values of planes K=3 (read back) and K=4 (this plane);
@@ -733,7 +738,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                             store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
                     if (STAGE == 3)
-                        cfl_acc_direct<MAG>(cfa, s, m, gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
+                        cfl_acc_direct<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
                 }
                 if (bot) {
                     // bottom wall: new values of planes K=NZ-2 and K=NZ-3, read back
@@ -754,7 +759,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                         else
                             store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
-                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
                 }
             }
         } else if (STAGE >= 2) {
@@ -762,7 +767,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
             zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
         }
         if (!zok) atomicOr(sflag, 1);
-        if (STAGE == 3) cfl_fold_plane(red, cfa, m.rkapa[k + 1]);
+        if (STAGE == 3) cfl_fold_plane(red, cfa, m.rkapa[k + 1], s);
         if (STAGE >= 2) {
             ++zfill;
             if (tid == 0) zpending = false;

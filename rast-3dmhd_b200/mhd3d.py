@@ -134,12 +134,15 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_closure_tendency_adjoint.argtypes = [vp, vp, vp, vp, vp]
     lib.mhd3d_ensemble_tune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_double)]
+    lib.mhd3d_ensemble_tile.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.mhd3d_ensemble_set_tile.argtypes = [vp, C.c_int32]
     lib.mhd3d_version.restype = C.c_char_p
     lib.mhd3d_set_stream.argtypes = [vp, vp]
     lib.mhd3d_step_async.argtypes = [vp, C.c_int32]
     lib.mhd3d_sync.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     lib.mhd3d_profile.argtypes = [vp, C.c_int32]
+    lib.mhd3d_set_wait_limit.argtypes = [vp, C.c_int64]
     lib.mhd3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     lib.mhd3d_cfl_noalloc.argtypes = [C.POINTER(Params)] + [vp] * 13 + [vp]
     return lib
@@ -308,6 +311,12 @@ class GpuSim:
         return {"status": st, "dt": dt.value, "timc": timc.value, "timt": timt.value,
                 "umach": umach.value, "nit": nit.value}
 
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the FP64 stage kernels' first ring wait (test use)."""
+        st = self.lib.mhd3d_set_wait_limit(self.h, polls)
+        if st:
+            raise Mhd3dError(st, "mhd3d_set_wait_limit")
+
     def profile(self, enable: bool = True):
         st = self.lib.mhd3d_profile(self.h, 1 if enable else 0)
         if st:
@@ -427,7 +436,23 @@ class Ensemble:
         st = self.lib.mhd3d_ensemble_tune(self.h, steps, C.byref(z), C.byref(c), C.byref(ms))
         if st:
             raise Mhd3dError(st, "mhd3d_ensemble_tune")
-        return {"zlen": z.value, "ctas_per_sm": c.value, "ms_per_step": ms.value}
+        tx, ty = C.c_int32(), C.c_int32()
+        st = self.lib.mhd3d_ensemble_tile(self.h, C.byref(tx), C.byref(ty))
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_tile")
+        return {"zlen": z.value, "ctas_per_sm": c.value, "ms_per_step": ms.value, "tile": [tx.value, ty.value]}
+
+    def set_tile(self, rows: int):
+        st = self.lib.mhd3d_ensemble_set_tile(self.h, rows)
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_set_tile")
+
+    def tile(self) -> list:
+        tx, ty = C.c_int32(), C.c_int32()
+        st = self.lib.mhd3d_ensemble_tile(self.h, C.byref(tx), C.byref(ty))
+        if st:
+            raise Mhd3dError(st, "mhd3d_ensemble_tile")
+        return [tx.value, ty.value]
 
 
 def par1_record(cfg: RunConfig, ncase=1, ncasep=1, ntotal=1000, nstep0=100, nstart=0, npe=1, npey=1, nit=0,

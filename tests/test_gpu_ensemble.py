@@ -73,11 +73,32 @@ def test_ensemble_tune_leaves_state(mhd3d):
         m.upload(su.state)
     ens.step(2)
     t = ens.tune(steps=2)
-    assert t["zlen"] in (4, 6, 8, 12, 16, 24, 32, 48, 64) and t["ctas_per_sm"] in (2, 3, 4)
-    assert t["ms_per_step"] > 0
+    # the search: tile rows 2, 4, 8 (32 columns) x z chunk x CTAs per SM
+    assert t["zlen"] in (4, 6, 8, 12, 16, 24, 32, 48, 64)
+    allowed = {2: (4, 6, 8), 4: (2, 3, 4), 8: (1, 2)}
+    assert t["tile"][0] == 32 and t["ctas_per_sm"] in allowed[t["tile"][1]], t
+    assert t["ms_per_step"] > 0 and ens.tile() == t["tile"]
     r = ens.step(3)
     assert list(r["nit"]) == [5] * len(setups)
     _check(mhd3d, ens, _singles(mhd3d, setups, 5))
+    ens.close()
+
+
+@pytest.mark.parametrize("rows", [2, 8])
+def test_ensemble_tile_shapes_give_the_same_bits(mhd3d, rows):
+    """The 32x2 and 32x8 tile instances against single-grid runs (32x4)."""
+    _gpu_or_skip(mhd3d)
+    setups = _setups(mhd3d)
+    ens = mhd3d.Ensemble(setups)
+    ens.set_tile(rows)
+    assert ens.tile() == [32, rows]
+    for m, su in zip(ens.members, setups):
+        m.upload(su.state)
+    r = ens.step(5)
+    assert list(r["nit"]) == [5] * len(setups)
+    _check(mhd3d, ens, _singles(mhd3d, setups, 5))
+    with pytest.raises(mhd3d.Mhd3dError):
+        ens.set_tile(3)
     ens.close()
 
 
