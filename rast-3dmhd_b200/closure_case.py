@@ -38,6 +38,7 @@ Usage: python closure_case.py [--fine 256 256 128] [--fac 4] [--spin 5.0]
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import sys
@@ -314,11 +315,40 @@ def gain_grid(spec):
     return cands
 
 
-def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf"):
+def eddy_factors(spec):
+    """Candidate (viscosity, conduction, magnetic diffusivity) factors of
+    "1,1.5:1.5:1,2": a bare number scales all three."""
+    out = []
+    for tok in spec.split(","):
+        v = [float(x) for x in tok.split(":")]
+        out.append(tuple(v * 3) if len(v) == 1 else tuple(v))
+    return out
+
+
+def eddy_setup(setup, factors):
+    """The coarse run's set-up with its diffusion coefficients multiplied by
+    (fv, ft, fm): viscosity 1/RE, conduction OCV/REPR and magnetic diffusivity
+    1/RM, with RE, REPR and RM (the CFL limits' forms) divided to match.  The
+    constant-coefficient eddy-diffusivity part of the closure: the coarse grid
+    resolves less of the cascade that drains the resolved scales."""
+    fv, ft, fm = factors
+    if (fv, ft, fm) == (1.0, 1.0, 1.0):
+        return setup
+    p = mhd3d.Params.from_buffer_copy(setup.params)
+    p.ore *= fv
+    p.re /= fv
+    p.repr /= ft
+    p.orm *= fm
+    p.rm /= fm
+    return dataclasses.replace(setup, params=p)
+
+
+def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.0, 1.0, 1.0)):
     """A coarse FP32 run from the held-out run's filtered start over the window; with
     net, the closure is attached with only the named term groups applied,
-    scaled by the gain after '@' (terms "stress+heat@0.5")."""
-    g = mhd3d.GpuSim(heldout["coarse_setup"], mode=mhd3d.MODE_FP32)
+    scaled by the gain after '@' (terms "stress+heat@0.5"); eddy multiplies
+    the coarse run's diffusion coefficients (eddy_setup)."""
+    g = mhd3d.GpuSim(eddy_setup(heldout["coarse_setup"], eddy), mode=mhd3d.MODE_FP32)
     g.upload(heldout["start"])
     if net is not None:
         gains = term_gains(terms)
@@ -439,6 +469,9 @@ def main(argv=None):
     ap.add_argument("--gain-terms", default="stress+heat+emf")
     ap.add_argument("--gain-grid", default=None,
                     help="per-group gains tried on the training window, e.g. 'stress+heat:0,0.25;emf:0,0.12'")
+    ap.add_argument("--eddy", default="1",
+                    help="eddy-diffusivity factors tried on the training window with every gain candidate: "
+                         "comma-separated, each 'f' or 'fv:ft:fm' (viscosity, conduction, magnetic diffusivity)")
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the trained network and the held-out run's window (.npz)")
     ap.add_argument("--load", default=None, help="skip the fine runs and training: read a --save file")
@@ -463,30 +496,46 @@ def main(argv=None):
         apri = a_priori(net, heldout, log)
         if args.save:
             save_case(args.save, net, heldout, tr, apri, val)
-    chosen = None
+    chosen, chosen_eddy = None, (1.0, 1.0, 1.0)
     cands = gain_grid(args.gain_grid) if args.gain_grid else (
         [f"{args.gain_terms}@{gv}" for gv in args.gains.split(",")] if args.gains else [])
-    if cands and val is not None:
-        # the gains are chosen on the training run's own window, never on the held-out run's
+    eddies = eddy_factors(args.eddy)
+    if (cands or len(eddies) > 1) and val is not None:
+        # gains and eddy factors are chosen on the training run's own window, never on the held-out run's
         scores = {}
-        for cand in cands:
-            run = coarse_phase(val, net, args, log, f"validate {cand}", cand)
-            err = rel_errors(run["profiles"], val["profiles"])
-            scores[cand] = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
-            log(f"gains {cand}: status {run['status']} mean(ke, fconv, me) error {scores[cand]}")
-        ok = {k: v for k, v in scores.items() if v is not None}
+        best = None
+        # with several eddy factors the plain coarse run (no network) competes as well
+        pool = (cands + [None]) if len(eddies) > 1 else (cands or [None])
+        for ed in eddies:
+            for cand in pool:
+                key = f"{cand}|eddy={':'.join(f'{x:g}' for x in ed)}"
+                run = coarse_phase(val, net if cand else None, args, log, f"validate {key}", cand or "", ed)
+                err = rel_errors(run["profiles"], val["profiles"])
+                sc = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
+                scores[key] = sc
+                log(f"{key}: status {run['status']} mean(ke, fconv, me) error {sc}")
+                if sc is not None and (best is None or sc < best[0]):
+                    best = (sc, cand, ed)
         plain_val = rel_errors(coarse_phase(val, None, args, log, "validate plain")["profiles"], val["profiles"])
-        chosen = min(ok, key=ok.get) if ok else None
+        if best is not None:
+            chosen, chosen_eddy = best[1], best[2]
         tr["gain_scores"] = scores
         tr["gain_plain_score"] = float(np.mean([plain_val[n] for n in ("ke", "fconv", "me")]))
         tr["gain_chosen"] = chosen
+        tr["eddy_chosen"] = list(chosen_eddy)
     runs = [("plain", coarse_phase(heldout, None, args, log, "plain"))]
     variants = args.variants.split(",") if args.variants else []
-    if chosen is not None:
-        variants.append(chosen)
     for v in variants:
         runs.append(("closure" if v == "stress+heat+emf" else f"closure[{v}]",
                      coarse_phase(heldout, net, args, log, f"closure[{v}]", v)))
+    if chosen_eddy != (1.0, 1.0, 1.0):
+        tag = f"eddy={':'.join(f'{x:g}' for x in chosen_eddy)}"
+        runs.append((f"plain[{tag}]", coarse_phase(heldout, None, args, log, f"plain[{tag}]", "", chosen_eddy)))
+        if chosen is not None:
+            runs.append((f"closure[{chosen}|{tag}]",
+                         coarse_phase(heldout, net, args, log, f"closure[{chosen}|{tag}]", chosen, chosen_eddy)))
+    elif chosen is not None:
+        runs.append((f"closure[{chosen}]", coarse_phase(heldout, net, args, log, f"closure[{chosen}]", chosen)))
     ref = heldout["profiles"]
     res = {
         "fine": list(args.fine), "fac": args.fac, "ra": args.ra, "ta": args.ta, "contrast": args.contrast,

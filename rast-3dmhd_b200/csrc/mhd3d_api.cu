@@ -1262,7 +1262,7 @@ int create(const mhd3d_params* p, const double* const arrs[14], void** out)
     const long ntiles = (long)h->ntx * ((npy + tyw - 1) / tyw);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
-    const long want = 2L * sms * (h->f32 ? 5 : MHD3D_MINB);   // CTAs resident per SM
+    const long want = 2L * sms * (h->f32 ? MHD3D_MINB32 : MHD3D_MINB);   // CTAs resident per SM
     int nch = (npz + MHD3D_ZCHUNK - 1) / MHD3D_ZCHUNK;
     const int fill = (int)std::min<long>((want + ntiles - 1) / ntiles, npz / 4);
     if (fill > nch) nch = fill;

@@ -130,6 +130,9 @@ struct StageArgs {
 #ifndef MHD3D_TY32
 #define MHD3D_TY32 4
 #endif
+#ifndef MHD3D_MINB32
+#define MHD3D_MINB32 5   // FP32 stage CTAs per SM: 5 x 128 threads x 96 registers, 5 x 34 KB shared
+#endif
 constexpr int TY32 = MHD3D_TY32;        // tile rows of the FP32 kernel
 constexpr int NT32 = TX * TY32;
 constexpr int BW32 = 36;                // TMA box row: x0-1 .. x0+34 (36 floats = 144 B, a 16-B multiple)

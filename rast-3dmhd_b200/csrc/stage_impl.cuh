@@ -42,7 +42,7 @@ enum Q { Q_RU = 0, Q_RV, Q_RW, Q_RO, Q_TT, Q_RI, Q_UU, Q_VV, Q_WW, Q_P, Q_BX, Q_
 // raw-plane ring slots: planes k-1, k, k+1 in use and, with 4, plane k+2 in
 // flight (with 3 the next plane is issued when plane k-1's slot frees)
 constexpr int NRAW = MHD3D_NRAW;
-static_assert(NRAW == 3 || NRAW == 4, "three or four ring slots");
+static_assert(NRAW >= 3 && NRAW <= 7, "three to seven ring slots");
 constexpr int NRI = 3;    // 1/RO ring slots (planes k-1, k, k+1)
 
 template <bool MAG>
@@ -52,12 +52,36 @@ struct Lay {
     static constexpr int ZT = NF * TY * TX;                                   // Z tile doubles
     static constexpr int RI_OFF = NRAW * RAW_SLOT;
     static constexpr int Z_OFF = ((RI_OFF + NRI * BSLOT) * 8 + 127) / 128 * 128 / 8;
-    static constexpr int BAR_OFF = Z_OFF + ZT;           // 5 mbarriers (8 B each)
+    static constexpr int BAR_OFF = Z_OFF + ZT;           // NRAW+1 <= 8 mbarriers (8 B each)
     static constexpr int RED_OFF = BAR_OFF + 8;          // CFL block reduction
     static constexpr int FLAG_OFF = RED_OFF + (NT / 32) * 8;   // 3 keys + a 40-byte screening record per warp
     static constexpr int TOTAL = FLAG_OFF + 2;
     static constexpr size_t BYTES = (size_t)TOTAL * 8 + 128;   // + alignment slack
 };
+
+#ifndef MHD3D_FASTRCP
+#define MHD3D_FASTRCP 1
+#endif
+#if MHD3D_FAST_BODY && MHD3D_FASTRCP
+// 1/x by two Newton-Raphson steps y <- y + y(1 - xy) from the approximate
+// reciprocal rcp.approx.ftz.f64 (each step squares the relative error, so
+// two reach the rounding level): within an ulp or so of the correctly rounded
+// 1/x for the positive normal densities it is used on.  The derive step of
+// every arriving plane runs between a copy wait and a CTA barrier, where a
+// full division's latency shows.  FMA build only; the reference-rounding
+// build divides.
+__device__ __forceinline__ double recip(double x)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+#else
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+#endif
 
 // value of quantity QQ at offset off of a plane slot: raw fields, 1/RO, and the
 // products FLUXES forms on the whole array (UU=RU*RO' with RO'=1/RO, WW1=RO*TT)
@@ -233,7 +257,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     auto derive_ri = [&](int kp) {
         const double* r = sraw + (size_t)((kp + 1) % NRAW) * L::RAW_SLOT + F_RO * BSLOT;
         double* d = sri + (size_t)((kp + 1) % 3) * BSLOT;
-        for (int p = tid; p < BSLOT; p += NT) d[p] = 1.0 / r[p];
+        for (int p = tid; p < BSLOT; p += NT) d[p] = recip(r[p]);
     };
 
     if (tid == 0)

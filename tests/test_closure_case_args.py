@@ -24,3 +24,20 @@ def test_gain_grid():
     assert c == ["stress@0+heat@0+emf@0", "stress@0+heat@0+emf@0.12",
                  "stress@0.25+heat@0.25+emf@0", "stress@0.25+heat@0.25+emf@0.12"]
     assert closure_case.term_gains(c[3]) == {"stress": 0.25, "heat": 0.25, "emf": 0.12}
+
+
+def test_eddy_factors():
+    assert closure_case.eddy_factors("1,1.5,2:1:1.5") == [(1.0, 1.0, 1.0), (1.5, 1.5, 1.5), (2.0, 1.0, 1.5)]
+
+
+def test_eddy_setup_scales_the_diffusion_coefficients():
+    import mhd3d
+    su = mhd3d.make_setup(mhd3d.convection_config(16, 16, 12))
+    assert closure_case.eddy_setup(su, (1.0, 1.0, 1.0)) is su
+    e = closure_case.eddy_setup(su, (2.0, 1.5, 3.0))
+    p, q = su.params, e.params
+    assert q.ore == p.ore * 2.0 and q.re == p.re / 2.0
+    assert q.repr == p.repr / 1.5
+    assert q.orm == p.orm * 3.0 and q.rm == p.rm / 3.0
+    assert q.npx == p.npx and q.ocv == p.ocv and q.grav == p.grav
+    assert e.grid is su.grid and e.state is su.state
