@@ -13,7 +13,7 @@
 #pragma once
 
 #ifndef MHD3D_MINB
-#define MHD3D_MINB 3   // FP64 stage CTAs per SM: 3 x 128 threads x 168 registers, 3 x 65 KB shared
+#define MHD3D_MINB 3   // FP64 stage CTAs per SM: 3 x 128 threads x 168 registers, 3 x 72 KB shared
 #endif
 #include <cuda.h>
 #include <cuda_runtime.h>

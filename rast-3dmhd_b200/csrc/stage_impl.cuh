@@ -42,7 +42,7 @@ enum Q { Q_RU = 0, Q_RV, Q_RW, Q_RO, Q_TT, Q_RI, Q_UU, Q_VV, Q_WW, Q_P, Q_BX, Q_
 // raw-plane ring slots: planes k-1, k, k+1 in use and, with 4, plane k+2 in
 // flight (with 3 the next plane is issued when plane k-1's slot frees)
 constexpr int NRAW = MHD3D_NRAW;
-static_assert(NRAW >= 3 && NRAW <= 7, "three to seven ring slots");
+static_assert(NRAW >= 3 && NRAW <= 6, "three to six ring slots (NRAW+2 mbarriers)");
 constexpr int NRI = 3;    // 1/RO ring slots (planes k-1, k, k+1)
 
 template <bool MAG>
@@ -52,7 +52,7 @@ struct Lay {
     static constexpr int ZT = NF * TY * TX;                                   // Z tile doubles
     static constexpr int RI_OFF = NRAW * RAW_SLOT;
     static constexpr int Z_OFF = ((RI_OFF + NRI * BSLOT) * 8 + 127) / 128 * 128 / 8;
-    static constexpr int BAR_OFF = Z_OFF + ZT;           // NRAW+1 <= 8 mbarriers (8 B each)
+    static constexpr int BAR_OFF = Z_OFF + 2 * ZT;       // two Z slots; NRAW+2 <= 8 mbarriers (8 B each)
     static constexpr int RED_OFF = BAR_OFF + 8;          // CFL block reduction
     static constexpr int FLAG_OFF = RED_OFF + (NT / 32) * 8;   // 3 keys + a 40-byte screening record per warp
     static constexpr int TOTAL = FLAG_OFF + 2;
@@ -168,7 +168,7 @@ __device__ __forceinline__ void cfl_commit(Accum* acc, unsigned long long k1, un
 // ---------------------------------------------------------------------------
 template <bool MAG, bool ROT, int STAGE>
 #ifndef MHD3D_MINB
-#define MHD3D_MINB 3   // CTAs per SM: 3 x 128 threads x 168 registers, 3 x 65 KB shared
+#define MHD3D_MINB 3   // CTAs per SM: 3 x 128 threads x 168 registers, 3 x 72 KB shared
 #endif
 __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant__ StageArgs a)
 {
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         const bool stopped = STAGE != 0 && ctl->stop;
         *sflag = stopped ? -1 : 0;
         if (!stopped) {
-            for (int i = 0; i < NRAW + 1; ++i) mbar_init(&bars[i], 1);
+            for (int i = 0; i < NRAW + 2; ++i) mbar_init(&bars[i], 1);
             fence_mbar_init();
         }
     }
@@ -260,8 +260,23 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         for (int p = tid; p < BSLOT; p += NT) d[p] = recip(r[p]);
     };
 
-    if (tid == 0)
+    // Z of plane kp (stages 2, 3) goes to slot (kp-k0)&1, a plane ahead of its
+    // use; it is the ((kp-k0)>>1)-th fill of that slot's barrier
+    int z_hi = k0 - 1;   // thread 0: highest Z plane issued so far
+    auto issue_z = [&](int kp) {
+        const int zs = (kp - k0) & 1;
+        fence_proxy_async();
+        mbar_expect_tx(&bars[NRAW + zs], z_bytes);
+        tma_load4(sz + (size_t)zs * L::ZT, &a.map_z, &bars[NRAW + zs], x0, y0, kp, 0);
+        z_hi = kp;
+    };
+    auto wait_z = [&](int kp) -> bool {
+        return mbar_wait(&bars[NRAW + ((kp - k0) & 1)], (unsigned)(((kp - k0) >> 1) & 1));
+    };
+    if (tid == 0) {
         for (int kp = k0 - 1; kp <= k0 - 2 + NRAW && kp <= k1; ++kp) issue_plane(kp);
+        if (STAGE >= 2) issue_z(k0);
+    }
     // the first wait's limit is a launch argument (a test lowers it to make
     // the wait give up); every other wait, the drain's included, is bounded
     // by WAIT_LIMIT
@@ -273,17 +288,11 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
     } else {
         atomicOr(sflag, 1);
     }
-    bool zpending = false;   // thread 0: a Z fill is in flight
-    int zfill = 0;           // fills of the Z barrier so far
     CflAcc cfa;              // stage-3 CFL parts of this thread's cells
 
     for (int k = k0; k < k1; ++k) {
-        if (STAGE >= 2 && tid == 0 && !*sflag) {
-            fence_proxy_async();
-            mbar_expect_tx(&bars[NRAW], z_bytes);
-            tma_load4(sz, &a.map_z, &bars[NRAW], x0, y0, k, 0);
-            zpending = true;
-        }
+        // Z of the next plane goes to the slot plane k-1's Z has left
+        if (STAGE >= 2 && tid == 0 && !*sflag && k + 1 < k1) issue_z(k + 1);
         if (!mbar_wait(&bars[(k + 2) % NRAW], parity_of(k + 1))) atomicOr(sflag, 1);
         else derive_ri(k + 1);
         __syncthreads();
@@ -682,8 +691,8 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                     zu = RUc; zv = RVc; zw = RWc; zr = ROc; zt = TTc;
                     if (MAG) { zbx = BXc0; zby = BYc0; zbz = BZc0; }
                 } else {
-                    zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
-                    const double* zt_ = sz + ty * TX + tx;
+                    zok = wait_z(k);
+                    const double* zt_ = sz + (size_t)((k - k0) & 1) * L::ZT + ty * TX + tx;
                     zu = zt_[F_RU * TY * TX];
                     zv = zt_[F_RV * TY * TX];
                     zw = zt_[F_RW * TY * TX];
@@ -787,15 +796,11 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                 }
             }
         } else if (STAGE >= 2) {
-            // columns outside the domain still consume the Z fill of this plane
-            zok = mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
+            // columns outside the domain still see the Z fill of this plane land
+            zok = wait_z(k);
         }
         if (!zok) atomicOr(sflag, 1);
         if (STAGE == 3) cfl_fold_plane(red, cfa, m.rkapa[k + 1], s);
-        if (STAGE >= 2) {
-            ++zfill;
-            if (tid == 0) zpending = false;
-        }
         __syncthreads();
         if (*sflag) break;
         // refill: plane k+NRAW-1 goes to the slot plane k-1 has left
@@ -808,7 +813,9 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
             // the last fill of each slot is one of the NRAW highest planes issued
             for (int kp = hi_issued - (NRAW - 1); kp <= hi_issued; ++kp)
                 if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) % NRAW], parity_of(kp));
-            if (zpending) mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
+            // and the last fill of each Z slot is one of the two highest Z planes issued
+            for (int kp = z_hi - 1; kp <= z_hi; ++kp)
+                if (kp >= k0) wait_z(kp);
             atomicExch(&a.ctl->status, MHD3D_ERR_TIMEOUT);
             atomicExch(&a.ctl->stop, 1);
         }
