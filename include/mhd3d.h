@@ -303,7 +303,10 @@ int mhd3d_ensemble_set_stream(void* ens, void* stream);
  * arrays are device pointers; activations are channels-last BF16
  * [nz][ny][nx][C] (periodic in x and y, zero outside in z), weights BF16
  * [cout][27*cin] with k = tap*cin + ci, tap = (dx+1) + 3*(dy+1) + 9*(dz+1).
- * nx must be a multiple of 128 or divide 128; every array is 16-byte aligned.
+ * Any nx >= 1 (x segments of 128 voxels; a segment that runs past the row's
+ * end, or a row shorter than 128, wraps periodically and stores only its own
+ * voxels; nx a multiple of 128 takes the TMA loader); every array is 16-byte
+ * aligned.
  * Supported (cin, cout): (16,32), (32,32),
  * (32,16).  Work is enqueued on stream; err (device int) is set non-zero if
  * a bounded wait of the tensor-core pipeline gave up.
@@ -327,7 +330,7 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
                        int32_t ny, int32_t nz, void* stream);
 
 /*
- * Learned closure on an FP32 handle whose NPX is a multiple of 128 or divides 128.
+ * Learned closure on an FP32 handle (any NPX).
  * mhd3d_closure_set attaches a trained network (weights BF16 [cout][27*cin]:
  * w1 32x432, w2 32x864, w3 16x864; biases FP32 32, 32, 16; in_scale[8] the
  * feature scales; out_scale[12] the target scales; host or device pointers,

@@ -213,6 +213,24 @@ class PairCollector:
         return out
 
 
+class EnsemblePairs:
+    """Training pairs from the members of an ensemble (grids of uneven sizes):
+    one PairCollector a member, on that member's coarse grid (coarse_setups[i],
+    the member's physics at 1/fac resolution)."""
+
+    def __init__(self, ens: mhd3d.Ensemble, coarse_setups, fac: int = 4):
+        self.members = ens.members
+        self.collectors = [PairCollector(m.setup, cs, fac=fac) for m, cs in zip(ens.members, coarse_setups)]
+
+    def snapshot(self, in_scale):
+        """[(features, targets, shape)] of every member's current state."""
+        return [pc.snapshot(m, in_scale) + (pc.shape,) for m, pc in zip(self.members, self.collectors)]
+
+    def close(self):
+        for pc in self.collectors:
+            pc.coarse.close()
+
+
 def tendencies(sim: mhd3d.GpuSim, pred, out_scale, trip: float = 1e30):
     """Closure tendencies [7, nz, ny, nx] (RU, RV, RW, TT, BX, BY, BZ) of pred for sim's state."""
     torch = _torch()

@@ -15,7 +15,10 @@
 //    channels and x a multiple of 128, 64-byte voxel rows in the copy
 //    engine's 64-byte swizzle (one TMA box per plane); otherwise
 //    [8-channel chunk][voxel] 16-byte rows, the canonical K-major no-swizzle
-//    layout with 8-row groups 128 bytes apart.  One MMA serves three output rows (N = 3*COUT,
+//    layout with 8-row groups 128 bytes apart.  Any nx: a tile that runs past
+//    the row's end reads the row again from its start (periodic), and only
+//    its first nx - x0 outputs are stored (for nx < 128 the tile holds the
+//    row's period more than once).  One MMA serves three output rows (N = 3*COUT,
 //    the y taps stacked in the B operand), see k_conv3d.  Warp roles: a
 //    loader (TMA boxes, or cp.async when nx is not a multiple of 128), one
 //    MMA thread and four epilogue warps, handing off through mbarriers.  The
@@ -989,7 +992,7 @@ extern "C" {
 int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const float* bias, const void* mask,
                  int32_t relu, void* y, float* yf, int32_t nx, int32_t ny, int32_t nz, int32_t* err, void* stream)
 {
-    if (!x || !w || !err || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0 || (!y && !yf))
+    if (!x || !w || !err || nx <= 0 || ny <= 0 || nz <= 0 || (!y && !yf))
         return MHD3D_ERR_ARG;
     if (!aligned16(x) || !aligned16(w) || !aligned16(mask) || !aligned16(y) || !aligned16(yf)) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1004,7 +1007,7 @@ int mhd3d_conv3d(int32_t cin, int32_t cout, const void* x, const void* w, const 
 int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, float* db, int32_t nx,
                        int32_t ny, int32_t nz, void* stream)
 {
-    if (!x || !dy || !dw || nx <= 0 || (nx % MT && MT % nx) || ny <= 0 || nz <= 0) return MHD3D_ERR_ARG;
+    if (!x || !dy || !dw || nx <= 0 || ny <= 0 || nz <= 0) return MHD3D_ERR_ARG;
     if (!aligned16(x) || !aligned16(dy)) return MHD3D_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e;

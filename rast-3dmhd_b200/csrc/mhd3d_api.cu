@@ -1648,7 +1648,7 @@ int closure_set(Handle* h, const void* const w[3], const float* const b[3], cons
         h->clo = false;
         return MHD3D_OK;
     }
-    if (!h->f32 || (h->p.npx % 128 && 128 % h->p.npx) || !w[1] || !w[2] || !b[0] || !b[1] || !b[2] || !in_scale || !out_scale)
+    if (!h->f32 || !w[1] || !w[2] || !b[0] || !b[1] || !b[2] || !in_scale || !out_scale)
         return MHD3D_ERR_ARG;
     const size_t nv = (size_t)h->p.npx * h->p.npy * h->p.npz;
     const size_t wn[3] = {32 * 27 * 16, 32 * 27 * 32, 16 * 27 * 32}, bn[3] = {32, 32, 16};

@@ -49,10 +49,12 @@ def test_bad_arguments_rejected_before_device_use(mhd3d):
     assert lib.mhd3d_step(None, 1, None, None, None, None, None) == 1
     assert lib.mhd3d_upload(None, *([None] * 8)) == 1
     assert lib.mhd3d_destroy(None) == 0
-    # closure convolutions: x periods that neither divide nor are multiples of 128
+    # closure convolutions: empty extents, a channel pair that is not built, missing outputs
     buf = C.create_string_buffer(64)
     p = C.cast(buf, C.c_void_p)
     err = C.cast(buf, C.POINTER(C.c_int32))
-    for nx in (0, 96, 200):
-        assert lib.mhd3d_conv3d(16, 32, p, p, None, None, 0, p, None, nx, 4, 4, err, None) == 1
-        assert lib.mhd3d_conv3d_wgrad(16, 32, p, p, C.cast(buf, C.POINTER(C.c_float)), None, nx, 4, 4, None) == 1
+    for nx, ny, nz in ((0, 4, 4), (96, 0, 4), (200, 4, -1)):
+        assert lib.mhd3d_conv3d(16, 32, p, p, None, None, 0, p, None, nx, ny, nz, err, None) == 1
+        assert lib.mhd3d_conv3d_wgrad(16, 32, p, p, C.cast(buf, C.POINTER(C.c_float)), None, nx, ny, nz, None) == 1
+    assert lib.mhd3d_conv3d(16, 16, p, p, None, None, 0, p, None, 96, 4, 4, err, None) == 1
+    assert lib.mhd3d_conv3d(16, 32, p, p, None, None, 0, None, None, 96, 4, 4, err, None) == 1

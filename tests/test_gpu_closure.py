@@ -27,9 +27,11 @@ def _p(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
-# x periods of 128 and 256, and 64 and 32: a 128-point tile then spans several periods
+# x periods of 128 and 256 (TMA rows); 64 and 32: a 128-point tile then spans
+# several periods; 96, 24, 160 and 200: tiles that wrap part of a period
 SHAPES = [((5, 6, 128), 16, 32), ((4, 3, 256), 32, 32), ((3, 5, 128), 32, 16),
-          ((4, 6, 64), 16, 32), ((3, 4, 32), 32, 32), ((5, 3, 64), 32, 16)]
+          ((4, 6, 64), 16, 32), ((3, 4, 32), 32, 32), ((5, 3, 64), 32, 16),
+          ((3, 4, 96), 16, 32), ((4, 3, 24), 32, 32), ((3, 3, 160), 32, 16), ((2, 3, 200), 32, 32)]
 
 
 @pytest.mark.parametrize("shape,cin,cout", SHAPES)

@@ -185,15 +185,16 @@ def test_tendency_loss_and_adjoint(mhd3d):
     g.close()
 
 
-def _coarse_setup(mhd3d):
-    return mhd3d.make_setup(mhd3d.convection_config(128, 16, 16, ra=1e5, ta=1e4, ampt=1e-2, seed=2))
+def _coarse_setup(mhd3d, npx=128):
+    return mhd3d.make_setup(mhd3d.convection_config(npx, 16, 16, ra=1e5, ta=1e4, ampt=1e-2, seed=2))
 
 
-def test_closure_fallback_is_the_plain_step(mhd3d):
+@pytest.mark.parametrize("npx", [128, 96, 24])
+def test_closure_fallback_is_the_plain_step(mhd3d, npx):
     _gpu_or_skip(mhd3d)
     pytest.importorskip("torch")
     import closure
-    setup = _coarse_setup(mhd3d)
+    setup = _coarse_setup(mhd3d, npx)
     plain = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
     plain.upload(setup.state)
     plain.step(12)
