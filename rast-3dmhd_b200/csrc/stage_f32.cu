@@ -35,12 +35,7 @@ namespace f32 {
 
 #include "cfl_acc.cuh"
 
-#ifndef MHD3D_NRAW32
-#define MHD3D_NRAW32 4
-#endif
-// raw-plane ring slots: planes k-1, k, k+1 in use and NRAW-3 planes in flight
-constexpr int NRAW = MHD3D_NRAW32;
-static_assert(NRAW >= 4 && NRAW <= 7, "four to seven ring slots");
+constexpr int NRAW = 4;
 constexpr int NRI = 3;
 
 constexpr size_t al128(size_t b) { return (b + 127) / 128 * 128; }
@@ -221,17 +216,17 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
 
     int hi_issued = k0 - 2;
     auto issue_plane = [&](int kp) {
-        const int sl = (kp + 1) % NRAW;
+        const int sl = (kp + 1) & 3;
         fence_proxy_async();
         mbar_expect_tx(&bars[sl], raw_bytes);
         tma_load4(reinterpret_cast<unsigned char*>(sraw) + (size_t)sl * L::RAW_SLOT_B, &a.map_u, &bars[sl], x0, y0,
                   kp + 1, 0);
         hi_issued = kp;
     };
-    auto parity_of = [&](int kp) -> unsigned { return (unsigned)(((kp - (k0 - 1)) / NRAW) & 1); };
+    auto parity_of = [&](int kp) -> unsigned { return (unsigned)(((kp - (k0 - 1)) >> 2) & 1); };
     auto slot = [&](int kp) -> const float* {
         return reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(sraw) +
-                                              (size_t)((kp + 1) % NRAW) * L::RAW_SLOT_B);
+                                              (size_t)((kp + 1) & 3) * L::RAW_SLOT_B);
     };
     auto derive_ri = [&](int kp) {
         const float* r = slot(kp) + F_RO * BSL;
@@ -241,8 +236,8 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
     };
 
     if (tid == 0)
-        for (int kp = k0 - 1; kp <= k0 + NRAW - 2 && kp <= k1; ++kp) issue_plane(kp);
-    bool ok = mbar_wait(&bars[(k0 + 0) % NRAW], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) % NRAW], parity_of(k0));
+        for (int kp = k0 - 1; kp <= k0 + 2 && kp <= k1; ++kp) issue_plane(kp);
+    bool ok = mbar_wait(&bars[(k0 + 0) & 3], parity_of(k0 - 1)) && mbar_wait(&bars[(k0 + 1) & 3], parity_of(k0));
     if (ok) {
         derive_ri(k0 - 1);
         derive_ri(k0);
@@ -264,7 +259,7 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
             tma_load4(sz, &a.map_z, &bars[NRAW], x0, y0, k, 0);
             zpending = true;
         }
-        if (!mbar_wait(&bars[(k + 2) % NRAW], parity_of(k + 1))) atomicOr(sflag, 1);
+        if (!mbar_wait(&bars[(k + 2) & 3], parity_of(k + 1))) atomicOr(sflag, 1);
         else derive_ri(k + 1);
         __syncthreads();
         if (*sflag) break;
@@ -590,12 +585,12 @@ __device__ __forceinline__ void stage32_item(const StageArgs32& a, const int til
         }
         __syncthreads();
         if (*sflag) break;
-        if (tid == 0 && k + NRAW - 1 <= k1) issue_plane(k + NRAW - 1);
+        if (tid == 0 && k + 3 <= k1) issue_plane(k + 3);
     }
     if (*sflag) {
         if (tid == 0) {
-            for (int kp = hi_issued - (NRAW - 1); kp <= hi_issued; ++kp)
-                if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) % NRAW], parity_of(kp));
+            for (int kp = hi_issued - 3; kp <= hi_issued; ++kp)
+                if (kp >= k0 - 1) mbar_wait(&bars[(kp + 1) & 3], parity_of(kp));
             if (zpending) mbar_wait(&bars[NRAW], (unsigned)(zfill & 1));
             atomicExch(&a.ctl->status, MHD3D_ERR_TIMEOUT);
             atomicExch(&a.ctl->stop, 1);

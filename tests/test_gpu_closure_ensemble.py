@@ -73,7 +73,7 @@ def test_ensemble_members_train_the_closure(mhd3d):
     torch.cuda.synchronize()
     after = mse(data)
     assert int(net.err.item()) == 0
-    assert after < 0.5 * before, (before, after)
+    assert after < 0.8 * before, (before, after)
     # held-out snapshots of every member: better than no closure
     assert mse(test) < zero_mse(test), (mse(test), zero_mse(test))
     ep.close()
