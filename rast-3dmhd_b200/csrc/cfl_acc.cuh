@@ -21,6 +21,20 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
     return v;
 }
 
+// Per-column CFL factors, formed once per thread instead of once per cell:
+// MIN(DDX(I), DDY(J)) and, for the screening, MAX(1/DDX, 1/DDY) in FP32.
+struct CflCol {
+    double dd;
+    float rdd;
+};
+__device__ __forceinline__ CflCol cfl_col(const Metrics& m, int gi, int gj, bool active)
+{
+    CflCol c;
+    c.dd = active ? dmin(m.ddx[gi + 1], m.ddy[gj + 1]) : 0.0;
+    c.rdd = active ? fmaxf(m.rddx_f[gi + 1], m.rddy_f[gj + 1]) : 0.0f;
+    return c;
+}
+
 #if MHD3D_FAST_BODY
 // Contracted form: W1=DD/(|u|+c_f) (SQRT(FAST2) of the reference is |u|+c_f
 // exactly, c_f**2=GAMMA*TT+B**2*OBETA/RO), reduced as max((|u|+c_f)/DD);
@@ -100,14 +114,14 @@ __device__ __forceinline__ void cfl_screen_init(unsigned long long* red, const A
 
 template <bool MAG>
 __device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const Metrics& m, const CflScreen* scr,
-                                             int gi, int gj, int kd, double ru, double rv, double rw, double ro,
-                                             double tt, double bx, double by, double bz)
+                                             const CflCol& col, int gi, int gj, int kd, double ru, double rv,
+                                             double rw, double ro, double tt, double bx, double by, double bz)
 {
     const double mm = ru * ru + rv * rv + rw * rw;
     const double a2r = MAG ? s.gamma * tt * ro + (bx * bx + by * by + bz * bz) * s.obeta : s.gamma * tt * ro;
-    const double dd = dmin(dmin(m.ddx[gi + 1], m.ddy[gj + 1]), m.ddz[kd + 1]);
+    const double dd = dmin(col.dd, m.ddz[kd + 1]);
     const double wv = dd * dd * ro * fmin(s.cw3, m.fw2z[kd + 1]);
-    const float rddf = fmaxf(fmaxf(m.rddx_f[gi + 1], m.rddy_f[gj + 1]), m.rddz_f[kd + 1]);
+    const float rddf = fmaxf(col.rdd, m.rddz_f[kd + 1]);
     const float sf = (sqrt_approx((float)mm) + sqrt_approx((float)(ro * a2r))) * rddf;
     const double w_hi = scr->w_hi, mg_lo = scr->mg_lo;
     const float s_lo = scr->s_lo;
@@ -135,10 +149,10 @@ __device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const 
 // the top wall's cells (formed in the pass of plane 3): nothing plane-bound
 template <bool MAG>
 __device__ __forceinline__ void cfl_acc_direct(CflAcc& c, const Scalars& s, const Metrics& m, const CflScreen* scr,
-                                               int gi, int gj, int kd, double ru, double rv, double rw, double ro,
-                                               double tt, double bx, double by, double bz)
+                                               const CflCol& col, int gi, int gj, int kd, double ru, double rv,
+                                               double rw, double ro, double tt, double bx, double by, double bz)
 {
-    cfl_acc_cell<MAG>(c, s, m, scr, gi, gj, kd, ru, rv, rw, ro, tt, bx, by, bz);
+    cfl_acc_cell<MAG>(c, s, m, scr, col, gi, gj, kd, ru, rv, rw, ro, tt, bx, by, bz);
 }
 
 // end of a plane (all lanes): when a cell of the warp was formed in FP64,
@@ -204,9 +218,9 @@ __device__ __forceinline__ void cfl_screen_init(unsigned long long*, const Accum
 __device__ __forceinline__ const CflScreen* cfl_screen_of(const unsigned long long*) { return nullptr; }
 
 template <bool MAG>
-__device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const Metrics& m, const CflScreen*, int gi,
-                                             int gj, int kd, double ru, double rv, double rw, double ro, double tt,
-                                             double bx, double by, double bz)
+__device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const Metrics& m, const CflScreen*,
+                                             const CflCol&, int gi, int gj, int kd, double ru, double rv, double rw,
+                                             double ro, double tt, double bx, double by, double bz)
 {
     double w1, x, w3, mach2;
     cfl_terms<MAG>(s, ru, rv, rw, ro, tt, bx, by, bz, cell_dd(m, gi, gj, kd), w1, x, w3, mach2);
@@ -221,8 +235,8 @@ __device__ __forceinline__ void cfl_acc_cell(CflAcc& c, const Scalars& s, const 
 // formed in the pass of plane 3)
 template <bool MAG>
 __device__ __forceinline__ void cfl_acc_direct(CflAcc& c, const Scalars& s, const Metrics& m, const CflScreen*,
-                                               int gi, int gj, int kd, double ru, double rv, double rw, double ro,
-                                               double tt, double bx, double by, double bz)
+                                               const CflCol&, int gi, int gj, int kd, double ru, double rv, double rw,
+                                               double ro, double tt, double bx, double by, double bz)
 {
     CflPart cp;
     cfl_cell<MAG>(s, ru, rv, rw, ro, tt, bx, by, bz, cell_dd(m, gi, gj, kd), m.rkapa[kd + 1], cp);

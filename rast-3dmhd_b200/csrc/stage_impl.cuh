@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
         atomicOr(sflag, 1);
     }
     CflAcc cfa;              // stage-3 CFL parts of this thread's cells
+    const CflCol ccol = cfl_col(m, gi, gj, active);
 
     for (int k = k0; k < k1; ++k) {
         // Z of the next plane goes to the slot plane k-1's Z has left
@@ -736,7 +737,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                 }
                 // ---- BCON (3dmhdsub.f:2751-2955) and the CFL parts of the next step
                 if (!top && !bot) {
-                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, k, nu, nv, nw, nr, nt, nbx, nby, nbz);
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), ccol, gi, gj, k, nu, nv, nw, nr, nt, nbx, nby, nbz);
                 }
                 if (k == 2 && k0 == 0) {
                     // top wall: new values of planes K=3 (read back) and K=4 (this plane);
@@ -771,7 +772,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                             store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
                     if (STAGE == 3)
-                        cfl_acc_direct<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
+                        cfl_acc_direct<MAG>(cfa, s, m, cfl_screen_of(red), ccol, gi, gj, 0, ru_w, rv_w, 0.0, w0_ro, tt_w, w0_bx, w0_by, bz_w);
                 }
                 if (bot) {
                     // bottom wall: new values of planes K=NZ-2 and K=NZ-3, read back
@@ -792,7 +793,7 @@ __global__ void __launch_bounds__(NT, MHD3D_MINB) k_stage(const __grid_constant_
                         else
                             store_cell<4>(pl, a.uf, ucol, hc, {F_RU, F_RV, F_RW, F_TT}, {ru_w, rv_w, 0.0, tt_w});
                     }
-                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
+                    if (STAGE == 3) cfl_acc_cell<MAG>(cfa, s, m, cfl_screen_of(red), ccol, gi, gj, k, ru_w, rv_w, 0.0, nr, tt_w, nbx, nby, bz_w);
                 }
             }
         } else if (STAGE >= 2) {
