@@ -177,7 +177,8 @@ def fine_phase(args, seed, collect, log):
     if not collect:
         pairs = [pair]   # the last pair: its filtered state is resident in the collector
     fine.close()
-    return {"start": start, "pairs": pairs, "resid": resid, "profiles": np.mean(profs, axis=0), "t0": t0,
+    return {"start": start, "pairs": pairs, "resid": resid, "profiles": np.mean(profs, axis=0),
+            "profiles_t": np.array(profs), "t0": t0,
             "t1": t_sample,
             "steps": wsteps, "wall": wwall, "spin_steps": steps, "dt_mean": float(np.mean(dts)),
             "umach_max": float(np.max(machs)), "pc": pc, "coarse_setup": cs}
@@ -384,6 +385,7 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
     if net is not None:
         out["closure"] = g.closure_status()
     out["profiles"] = np.mean(profs, axis=0)
+    out["profiles_t"] = np.array(profs)
     g.close()
     return out
 
@@ -405,6 +407,8 @@ def save_case(path, net, heldout, tr, apri, val=None):
     d["in_scale"] = net.in_scale.cpu().numpy()
     d["out_scale"] = net.out_scale.cpu().numpy()
     d["profiles"] = heldout["profiles"]
+    if "profiles_t" in heldout:
+        d["profiles_t"] = heldout["profiles_t"]
     d["meta"] = np.array(json.dumps({k: heldout[k] for k in WINDOW_KEYS} | {"train": tr, "a_priori": apri}))
     np.savez(path, **d)
 
@@ -425,6 +429,8 @@ def load_case(path, args):
     start = {f: (z[f"start_{f}"] if f"start_{f}" in z else None) for f in mhd3d.FIELDS}
     heldout = {k: meta[k] for k in WINDOW_KEYS}
     heldout.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
+    if "profiles_t" in z:
+        heldout["profiles_t"] = z["profiles_t"]
     val = None
     if "val_profiles" in z:
         val = json.loads(str(z["val_meta"]))
@@ -544,8 +550,14 @@ def main(argv=None):
                         "spin_steps": heldout["spin_steps"], "umach_max": heldout["umach_max"]},
         "train": tr, "a_priori": apri,
     }
+    ke = mhd3d.PROFILES.index("ke")
     for name, run in runs:
-        d = {k: v for k, v in run.items() if k != "profiles"}
+        d = {k: v for k, v in run.items() if not k.startswith("profiles")}
+        ref_t = heldout.get("profiles_t")
+        if ref_t is not None and len(ref_t) == len(run["profiles_t"]):
+            # the run's volume KE over the filtered fine run's, sample by sample
+            d["ke_ratio_t"] = [float(a[ke].sum() / max(b[ke].sum(), 1e-300))
+                               for a, b in zip(run["profiles_t"], ref_t)]
         d["profile_rel_err"] = rel_errors(run["profiles"], ref)
         d["profile_rel_bias"] = {n: float((run["profiles"][i] - ref[i]).sum() / max(abs(ref[i].sum()), 1e-300))
                                  for i, n in enumerate(mhd3d.PROFILES)}
