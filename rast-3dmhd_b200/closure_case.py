@@ -125,9 +125,9 @@ def residual_target(pc, fine, nsteps):
 
 def fine_phase(args, seed, collect, log):
     """Spin up a fine run, then sample the window.  Returns the filtered
-    coarse state at the window start, the sampled pairs (all of them if
-    collect, else the last), the time-averaged filtered profiles and the
-    window's cost."""
+    coarse state the coarse runs start from (at the window start, or
+    ``--settle`` earlier), the sampled pairs (all of them if collect, else the
+    last), the time-averaged filtered profiles and the window's cost."""
     torch = _torch()
     fnx, fny, fnz = args.fine
     fac = args.fac
@@ -137,14 +137,28 @@ def fine_phase(args, seed, collect, log):
     fine.upload(fs.state)
     pc = closure.PairCollector(fs, cs, fac=fac)
     ones = torch.ones(8, dtype=torch.float32, device="cuda")
-    steps, _, r = advance_to(fine, args.spin, args.chunk, log, f"fine{seed} spin")
+    start, t_start = None, None
+    if args.settle > 0:
+        # the coarse runs start from the filtered state settle earlier and
+        # settle before the window: a filtered state is not in balance on the
+        # coarse grid, and its adjustment would otherwise fall in the window
+        steps, _, r = advance_to(fine, args.spin - args.settle, args.chunk, log, f"fine{seed} spin")
+        if r["status"]:
+            raise mhd3d.Mhd3dError(r["status"], "fine spin-up")
+        pc.snapshot(fine, ones)
+        start, t_start = pc.coarse_state(), r["timt"]
+        n, _, r = advance_to(fine, args.spin, args.chunk, log, f"fine{seed} spin", last=r)
+        steps += n
+    else:
+        steps, _, r = advance_to(fine, args.spin, args.chunk, log, f"fine{seed} spin")
     if r["status"]:
         raise mhd3d.Mhd3dError(r["status"], "fine spin-up")
     t0 = r["timt"]
     pairs, profs, resid = [], [], []
     pair = pc.snapshot(fine, ones)
     pc.t_last = r["timt"]
-    start = pc.coarse_state()
+    if start is None:
+        start, t_start = pc.coarse_state(), t0
     profs.append(pc.coarse.profiles())
     if collect:
         pairs.append(pair)
@@ -178,7 +192,7 @@ def fine_phase(args, seed, collect, log):
         pairs = [pair]   # the last pair: its filtered state is resident in the collector
     fine.close()
     return {"start": start, "pairs": pairs, "resid": resid, "profiles": np.mean(profs, axis=0),
-            "profiles_t": np.array(profs), "t0": t0,
+            "profiles_t": np.array(profs), "t0": t0, "t_start": t_start,
             "t1": t_sample,
             "steps": wsteps, "wall": wwall, "spin_steps": steps, "dt_mean": float(np.mean(dts)),
             "umach_max": float(np.max(machs)), "pc": pc, "coarse_setup": cs}
@@ -364,11 +378,23 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
     steps, wall, dts = 1, 0.0, []
     status, t_end = 0, 0.0
     span = heldout["t1"] - heldout["t0"]
+    lead = heldout["t0"] - (heldout.get("t_start") or heldout["t0"])
     t0 = time.perf_counter()
     r = g.step(1, check=False)
     wall += time.perf_counter() - t0
     tbase = r["timt"] - r["dt"]
-    for s in range(1, args.samples + 1):
+    if lead > 0 and not r["status"]:
+        # settle from the earlier filtered state up to the window (its steps
+        # and wall time count); the window's first sample is taken there
+        n, w, r = advance_to(g, tbase + lead, args.chunk, last=r)
+        steps += n
+        wall += w
+        tbase += lead
+        profs = [g.profiles()]
+    if r["status"]:
+        status, t_end = r["status"], r["timt"] - tbase
+        log(f"{tag} stopped while settling: status {status}")
+    for s in range(1, args.samples + 1 if not status else 1):
         n, w, r = advance_to(g, tbase + span * s / args.samples, args.chunk, last=r)
         steps += n
         wall += w
@@ -390,7 +416,7 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
     return out
 
 
-WINDOW_KEYS = ("t0", "t1", "steps", "wall", "spin_steps", "dt_mean", "umach_max")
+WINDOW_KEYS = ("t0", "t1", "t_start", "steps", "wall", "spin_steps", "dt_mean", "umach_max")
 
 
 def save_case(path, net, heldout, tr, apri, val=None):
@@ -427,7 +453,7 @@ def load_case(path, args):
     fnx, fny, fnz = args.fine
     cs = mhd3d.make_setup(config(fnx // args.fac, fny // args.fac, fnz // args.fac, args, args.heldout_seed))
     start = {f: (z[f"start_{f}"] if f"start_{f}" in z else None) for f in mhd3d.FIELDS}
-    heldout = {k: meta[k] for k in WINDOW_KEYS}
+    heldout = {k: meta.get(k) for k in WINDOW_KEYS}
     heldout.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
     if "profiles_t" in z:
         heldout["profiles_t"] = z["profiles_t"]
@@ -456,6 +482,9 @@ def main(argv=None):
     ap.add_argument("--ampt", type=float, default=5e-2)
     ap.add_argument("--spin", type=float, default=5.0)
     ap.add_argument("--window", type=float, default=2.0)
+    ap.add_argument("--settle", type=float, default=0.0,
+                    help="start the coarse runs from the filtered fine state this much simulated time before the "
+                         "window (it counts in their steps and wall time); 0: at the window start")
     ap.add_argument("--samples", type=int, default=16)
     ap.add_argument("--chunk", type=int, default=400)
     ap.add_argument("--iters", type=int, default=3000)
@@ -545,7 +574,7 @@ def main(argv=None):
     ref = heldout["profiles"]
     res = {
         "fine": list(args.fine), "fac": args.fac, "ra": args.ra, "ta": args.ta, "contrast": args.contrast,
-        "window": [heldout["t0"], heldout["t1"]],
+        "window": [heldout["t0"], heldout["t1"]], "settle": heldout["t0"] - (heldout.get("t_start") or heldout["t0"]),
         "fine_window": {"steps": heldout["steps"], "wall_s": heldout["wall"], "dt_mean": heldout["dt_mean"],
                         "spin_steps": heldout["spin_steps"], "umach_max": heldout["umach_max"]},
         "train": tr, "a_priori": apri,

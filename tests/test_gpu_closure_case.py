@@ -13,8 +13,8 @@ from test_gpu_parity import _gpu_or_skip
 pytestmark = pytest.mark.gpu
 
 ARGS = ["--fine", "64", "64", "32", "--ra", "1e5", "--ta", "1e4", "--contrast", "3", "--spin", "0.02",
-        "--window", "0.06", "--samples", "3", "--chunk", "50", "--iters", "30", "--resid-steps", "2",
-        "--resid-iters", "30", "--gains", "1,0.5"]
+        "--settle", "0.01", "--window", "0.06", "--samples", "3", "--chunk", "50", "--iters", "30",
+        "--resid-steps", "2", "--resid-iters", "30", "--gains", "1,0.5"]
 
 
 def test_closure_case_small(mhd3d, tmp_path):
@@ -26,6 +26,7 @@ def test_closure_case_small(mhd3d, tmp_path):
     res = closure_case.main(ARGS + ["--save", saved])
     assert res["fine"] == [64, 64, 32]
     assert res["window"][1] > res["window"][0]
+    assert 0 < res["settle"] < 0.02   # the coarse runs start from the filtered state before the window
     assert res["train"]["pairs"] == 4 and res["train"]["residual"]["pairs"] == 4
     assert set(res["a_priori"]) == {"commutator_error_ratio", "residual_error_ratio", "commutator_vs_residual_ratio"}
     assert res["train"]["gain_chosen"] in ("stress+heat+emf@1", "stress+heat+emf@0.5")
