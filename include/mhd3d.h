@@ -357,6 +357,18 @@ int mhd3d_conv3d_wgrad(int32_t cin, int32_t cout, const void* x, const void* dy,
 int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void* w2, const float* b2, const void* w3,
                       const float* b3, const float* in_scale, const float* out_scale, float trip);
 int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* err);
+/*
+ * A per-plane bias the attached closure adds to its tendencies (no
+ * counterpart in the reference): bias[f*NPZ + k] for the fields RU, RV, RW,
+ * TT, BX, BY, BZ (f = 0..6) and the interior planes k = 0..NPZ-1 (zero on
+ * the walls, which take no tendency), a host or device array of 7*NPZ
+ * floats, copied.  It is applied only on steps where the closure is (a step
+ * that falls back to the plain coarse method takes neither).  Meant for the
+ * horizontally uniform part of the coarse scheme's residual: the mismatch
+ * between a box-filtered state and the coarse grid's own discrete balance.
+ * NULL removes it.  FP32 handles only.
+ */
+int mhd3d_closure_set_bias(void* handle, const float* bias);
 int mhd3d_coarsen(void* fine, int32_t fac, double* cstate, float* targets, void* stream);
 int mhd3d_closure_features(void* handle, const float* in_scale, void* feat, double* means, void* stream);
 int mhd3d_closure_loss(const float* pred, const float* target, int64_t nvox, void* dy, double* loss, void* stream);

@@ -233,6 +233,10 @@ def train_residual(net, data, resid, pc, args, log):
     the network's outputs are fitted to R by the tendency loss (fields
     weighted by 1 / mean R_f^2) and its adjoint."""
     torch = _torch()
+    if args.bias:
+        # the per-plane bias takes the horizontally uniform part of the
+        # residual; the network is fitted to the rest
+        resid = [(R - R.mean(dim=(2, 3), keepdim=True), ca) for R, ca in resid]
     msq = torch.stack([(R.double() ** 2).mean(dim=(1, 2, 3)) for R, _ in resid]).mean(dim=0)
     w = (1.0 / msq.clamp_min(1e-300)).float()
     w = (w * 7.0 / w.sum()).contiguous()
@@ -259,6 +263,17 @@ def train_residual(net, data, resid, pc, args, log):
     torch.cuda.synchronize()
     return {"iters": args.resid_iters, "pairs": n, "loss_first": first, "loss_last": loss.item(),
             "seconds": time.perf_counter() - t0, "weights": w.cpu().tolist()}, w
+
+
+def residual_bias(resid):
+    """The horizontally uniform part of the coarse scheme's residual, averaged
+    over the training pairs: [7, NPZ] float32 on the device (RU, RV, RW, TT,
+    BX, BY, BZ; zero on the wall planes, as the targets are).  A box filter
+    on a stretched grid does not place the filtered mean profile where the
+    coarse grid's own discrete balance has it; this is the steady forcing
+    that mismatch leaves."""
+    torch = _torch()
+    return torch.stack([R.double().mean(dim=(2, 3)) for R, _ in resid]).mean(dim=0).float().contiguous()
 
 
 def a_priori(net, heldout, log):
@@ -358,13 +373,18 @@ def eddy_setup(setup, factors):
     return dataclasses.replace(setup, params=p)
 
 
-def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.0, 1.0, 1.0)):
+def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.0, 1.0, 1.0), bias=None):
     """A coarse FP32 run from the held-out run's filtered start over the window; with
     net, the closure is attached with only the named term groups applied,
-    scaled by the gain after '@' (terms "stress+heat@0.5"); eddy multiplies
-    the coarse run's diffusion coefficients (eddy_setup)."""
+    scaled by the gain after '@' (terms "stress+heat@0.5"), and with bias its
+    per-plane bias tendency ([7, NPZ]); eddy multiplies the coarse run's
+    diffusion coefficients (eddy_setup)."""
     g = mhd3d.GpuSim(eddy_setup(heldout["coarse_setup"], eddy), mode=mhd3d.MODE_FP32)
     g.upload(heldout["start"])
+    if terms.endswith("|bias"):
+        terms = terms[:-len("|bias")]
+    else:
+        bias = None
     if net is not None:
         gains = term_gains(terms)
         keep = net.out_scale
@@ -374,6 +394,8 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
         net.out_scale = sc
         net.attach(g, trip=args.trip)
         net.out_scale = keep
+        if bias is not None:
+            g.closure_set_bias(bias)
     profs = [g.profiles()]
     steps, wall, dts = 1, 0.0, []
     status, t_end = 0, 0.0
@@ -419,7 +441,7 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
 WINDOW_KEYS = ("t0", "t1", "t_start", "steps", "wall", "spin_steps", "dt_mean", "umach_max")
 
 
-def save_case(path, net, heldout, tr, apri, val=None):
+def save_case(path, net, heldout, tr, apri, val=None, bias=None):
     """The trained network and what the coarse runs are scored on (and, with
     val, the training run's window for choosing a gain)."""
     d = {f"start_{f}": a for f, a in heldout["start"].items() if a is not None}
@@ -433,6 +455,8 @@ def save_case(path, net, heldout, tr, apri, val=None):
     d["in_scale"] = net.in_scale.cpu().numpy()
     d["out_scale"] = net.out_scale.cpu().numpy()
     d["profiles"] = heldout["profiles"]
+    if bias is not None:
+        d["bias"] = bias.cpu().numpy()
     if "profiles_t" in heldout:
         d["profiles_t"] = heldout["profiles_t"]
     d["meta"] = np.array(json.dumps({k: heldout[k] for k in WINDOW_KEYS} | {"train": tr, "a_priori": apri}))
@@ -457,6 +481,8 @@ def load_case(path, args):
     heldout.update({"start": start, "profiles": z["profiles"], "coarse_setup": cs})
     if "profiles_t" in z:
         heldout["profiles_t"] = z["profiles_t"]
+    if "bias" in z:
+        heldout["bias"] = torch.tensor(z["bias"], device="cuda")
     val = None
     if "val_profiles" in z:
         val = json.loads(str(z["val_meta"]))
@@ -507,6 +533,10 @@ def main(argv=None):
     ap.add_argument("--eddy", default="1",
                     help="eddy-diffusivity factors tried on the training window with every gain candidate: "
                          "comma-separated, each 'f' or 'fv:ft:fm' (viscosity, conduction, magnetic diffusivity)")
+    ap.add_argument("--bias", action="store_true",
+                    help="fit the closure's per-plane bias tendency to the training run's horizontal-mean residual "
+                         "and the network to the rest; try every gain candidate with and without the bias, and the "
+                         "bias alone")
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the trained network and the held-out run's window (.npz)")
     ap.add_argument("--load", default=None, help="skip the fine runs and training: read a --save file")
@@ -515,25 +545,31 @@ def main(argv=None):
     def log(msg):
         print(msg, file=sys.stderr, flush=True)
 
-    val = None
+    val, bias = None, None
     if args.load:
         net, heldout, tr, apri, val = load_case(args.load, args)
+        bias = heldout.pop("bias", None)
     else:
         trainer = fine_phase(args, args.train_seed, True, log)
         net, tr, data = train(trainer["pairs"], args, log)
         val = {k: trainer[k] for k in WINDOW_KEYS + ("start", "profiles", "coarse_setup")}
         w = None
         if args.resid_steps:
+            bias = residual_bias(trainer["resid"])
             tr["residual"], w = train_residual(net, data, trainer["resid"], trainer["pc"], args, log)
         del trainer, data
         heldout = fine_phase(args, args.heldout_seed, False, log)
         heldout["resid_w"] = w
         apri = a_priori(net, heldout, log)
         if args.save:
-            save_case(args.save, net, heldout, tr, apri, val)
+            save_case(args.save, net, heldout, tr, apri, val, bias)
     chosen, chosen_eddy = None, (1.0, 1.0, 1.0)
     cands = gain_grid(args.gain_grid) if args.gain_grid else (
         [f"{args.gain_terms}@{gv}" for gv in args.gains.split(",")] if args.gains else [])
+    if args.bias and bias is not None and cands:
+        # every candidate again with the per-plane bias, and the bias alone
+        zero = "+".join(f"{g}@0" for g in TERMS)
+        cands = list(dict.fromkeys(cands + [c + "|bias" for c in cands] + [zero + "|bias"]))
     eddies = eddy_factors(args.eddy)
     if (cands or len(eddies) > 1) and val is not None:
         # gains and eddy factors are chosen on the training run's own window, never on the held-out run's
@@ -544,7 +580,7 @@ def main(argv=None):
         for ed in eddies:
             for cand in pool:
                 key = f"{cand}|eddy={':'.join(f'{x:g}' for x in ed)}"
-                run = coarse_phase(val, net if cand else None, args, log, f"validate {key}", cand or "", ed)
+                run = coarse_phase(val, net if cand else None, args, log, f"validate {key}", cand or "", ed, bias)
                 err = rel_errors(run["profiles"], val["profiles"])
                 sc = float(np.mean([err[n] for n in ("ke", "fconv", "me")])) if run["status"] == 0 else None
                 scores[key] = sc
@@ -568,9 +604,11 @@ def main(argv=None):
         runs.append((f"plain[{tag}]", coarse_phase(heldout, None, args, log, f"plain[{tag}]", "", chosen_eddy)))
         if chosen is not None:
             runs.append((f"closure[{chosen}|{tag}]",
-                         coarse_phase(heldout, net, args, log, f"closure[{chosen}|{tag}]", chosen, chosen_eddy)))
+                         coarse_phase(heldout, net, args, log, f"closure[{chosen}|{tag}]", chosen, chosen_eddy,
+                                      bias)))
     elif chosen is not None:
-        runs.append((f"closure[{chosen}]", coarse_phase(heldout, net, args, log, f"closure[{chosen}]", chosen)))
+        runs.append((f"closure[{chosen}]", coarse_phase(heldout, net, args, log, f"closure[{chosen}]", chosen,
+                                                        bias=bias)))
     ref = heldout["profiles"]
     res = {
         "fine": list(args.fine), "fac": args.fac, "ra": args.ra, "ta": args.ta, "contrast": args.contrast,

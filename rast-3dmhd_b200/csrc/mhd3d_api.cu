@@ -64,6 +64,7 @@ struct Handle {
     float *cb[3] = {nullptr, nullptr, nullptr}, *cin_scale = nullptr, *cout_scale = nullptr;
     __nv_bfloat16 *cfeat = nullptr, *cact1 = nullptr, *cact2 = nullptr;
     float *cpred = nullptr, *cfcl = nullptr;
+    float* cbias = nullptr;   // closure: per-plane bias tendency [7][NPZ] (null: none)
     double* cmeans = nullptr;                  // 3 x NPZ horizontal means (T, RO, BY)
     double* hpart = nullptr;                   // 3 x NPZ x HM_SPLIT partial sums of those means
     int* cflag = nullptr;                      // [0] trip flag of the current evaluation, [1] trips, [2] evaluations, [3] kernel error
@@ -577,8 +578,9 @@ constexpr size_t TEND_SMEM = (size_t)4 * TPV * 12 * sizeof(float);
 __global__ void __launch_bounds__(TTX * TTY) k_tendency(UView v, const float* __restrict__ pred,
                                                        const float* __restrict__ osc, const double* __restrict__ fax,
                                                        const double* __restrict__ fay, const double* __restrict__ faz,
-                                                       int npx, int npy, int npz, float trip, float* __restrict__ out,
-                                                       size_t fstride, size_t kstride, size_t jstride, int* flag)
+                                                       const float* __restrict__ bias, int npx, int npy, int npz,
+                                                       float trip, float* __restrict__ out, size_t fstride,
+                                                       size_t kstride, size_t jstride, int* flag)
 {
     extern __shared__ __align__(16) float tsm[];   // [slot 0..3][TPV][12], plane p in slot p & 3
     const int tid = threadIdx.x, tx = tid % TTX, ty = tid / TTX;
@@ -649,21 +651,26 @@ __global__ void __launch_bounds__(TTX * TTY) k_tendency(UView v, const float* __
                 auto dx = [&](int c) { return (xp[c] - xm[c]) * s[c] * ax; };
                 auto dy = [&](int c) { return (yp[c] - ym[c]) * s[c] * ay; };
                 auto dz = [&](int c) { return (zp[c] - zm[c]) * s[c] * az; };
-                o[0 * fstride] = -(dx(0) + dy(3) + dz(4));
-                o[1 * fstride] = -(dx(3) + dy(1) + dz(5));
-                o[2 * fstride] = -(dx(4) + dy(5) + dz(2));
-                o[3 * fstride] = -(dx(6) + dy(7) + dz(8)) / (float)ro;
-                o[4 * fstride] = dy(11) - dz(10);
-                o[5 * fstride] = dz(9) - dx(11);
-                o[6 * fstride] = dx(10) - dy(9);
+                float bz[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (bias) {
+#pragma unroll
+                    for (int f = 0; f < 7; ++f) bz[f] = bias[(size_t)f * npz + k];
+                }
+                o[0 * fstride] = -(dx(0) + dy(3) + dz(4)) + bz[0];
+                o[1 * fstride] = -(dx(3) + dy(1) + dz(5)) + bz[1];
+                o[2 * fstride] = -(dx(4) + dy(5) + dz(2)) + bz[2];
+                o[3 * fstride] = -(dx(6) + dy(7) + dz(8)) / (float)ro + bz[3];
+                o[4 * fstride] = dy(11) - dz(10) + bz[4];
+                o[5 * fstride] = dz(9) - dx(11) + bz[5];
+                o[6 * fstride] = dx(10) - dy(9) + bz[6];
             }
         }
         if (k + 2 <= kc1) store_plane(k + 2);   // slot of plane k-2, read by no thread since the last barrier
     }
 }
 
-cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const Metrics& m, int npx, int npy,
-                            int npz, float trip, float* out, size_t fstride, size_t kstride, size_t jstride,
+cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const Metrics& m, const float* bias, int npx,
+                            int npy, int npz, float trip, float* out, size_t fstride, size_t kstride, size_t jstride,
                             int* flag, cudaStream_t st)
 {
     static std::atomic<unsigned long long> attr{0};
@@ -671,7 +678,7 @@ cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const 
     if (ae != cudaSuccess) return ae;
     const dim3 grid((unsigned)((npx + TTX - 1) / TTX), (unsigned)((npy + TTY - 1) / TTY),
                     (unsigned)((npz + TZC - 1) / TZC));
-    k_tendency<<<grid, TTX * TTY, TEND_SMEM, st>>>(v, pred, osc, m.fax, m.fay, m.faz, npx, npy, npz, trip, out,
+    k_tendency<<<grid, TTX * TTY, TEND_SMEM, st>>>(v, pred, osc, m.fax, m.fay, m.faz, bias, npx, npy, npz, trip, out,
                                                   fstride, kstride, jstride, flag);
     return cudaGetLastError();
 }
@@ -967,6 +974,7 @@ int destroy(Handle* h)
     cudaFree(h->pb);
     cudaFree(h->cxy);
     cudaFree(h->cbuf);
+    cudaFree(h->cbias);
     cudaFree(h->ctl);
     cudaFree(h->acc);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -1632,7 +1640,7 @@ int closure_eval(Handle* h, int cur)
         mhd3d_conv3d(32, 32, h->cact1, h->cw[1], h->cb[1], nullptr, 1, h->cact2, nullptr, npx, npy, npz, err, h->st) ||
         mhd3d_conv3d(32, 16, h->cact2, h->cw[2], h->cb[2], nullptr, 0, nullptr, h->cpred, npx, npy, npz, err, h->st))
         return MHD3D_ERR_CUDA;
-    CK(launch_tendency(v, h->cpred, h->cout_scale, h->m, npx, npy, npz, h->ctrip, h->cfcl, h->zf, h->zz,
+    CK(launch_tendency(v, h->cpred, h->cout_scale, h->m, h->cbias, npx, npy, npz, h->ctrip, h->cfcl, h->zf, h->zz,
                        (size_t)h->zpitch, h->cflag, h->st));
     k_trip_count<<<1, 1, 0, h->st>>>(h->cflag);
     CK(cudaGetLastError());
@@ -2211,6 +2219,24 @@ int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void*
     return closure_set(static_cast<Handle*>(handle), w, b, in_scale, out_scale, trip);
 }
 
+int mhd3d_closure_set_bias(void* handle, const float* bias)
+{
+    Handle* h = static_cast<Handle*>(handle);
+    if (!h || !h->f32) return MHD3D_ERR_ARG;
+    CK(cudaSetDevice(h->dev));
+    if (int st = settle(h)) return st;
+    if (!bias) {
+        cudaFree(h->cbias);
+        h->cbias = nullptr;
+        return MHD3D_OK;
+    }
+    const size_t n = (size_t)7 * h->p.npz;
+    if (!h->cbias) CK(cudaMalloc(&h->cbias, n * sizeof(float)));
+    CK(cudaMemcpyAsync(h->cbias, bias, n * sizeof(float), cudaMemcpyDefault, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return MHD3D_OK;
+}
+
 int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* err)
 {
     Handle* h = static_cast<Handle*>(handle);
@@ -2288,7 +2314,7 @@ int mhd3d_closure_tendency(void* handle, const float* pred, const float* out_sca
     CK(cudaStreamSynchronize(h->st));
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t nv = (size_t)npx * npy * npz;
-    CK(launch_tendency(uview(h, h->cur), pred, out_scale, h->m, npx, npy, npz, trip, out, nv, (size_t)npx * npy,
+    CK(launch_tendency(uview(h, h->cur), pred, out_scale, h->m, nullptr, npx, npy, npz, trip, out, nv, (size_t)npx * npy,
                        (size_t)npx, flag, static_cast<cudaStream_t>(stream)));
     return MHD3D_OK;
 }

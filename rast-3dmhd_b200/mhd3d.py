@@ -125,6 +125,7 @@ def gpu_lib() -> C.CDLL:
     lib.mhd3d_conv3d_wgrad.argtypes = [i32, i32, vp, vp, vp, vp, i32, i32, i32, vp]
     lib.mhd3d_closure_set.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_float]
     lib.mhd3d_closure_status.argtypes = [vp, vp, vp, vp]
+    lib.mhd3d_closure_set_bias.argtypes = [vp, vp]
     lib.mhd3d_coarsen.argtypes = [vp, i32, vp, vp, vp]
     lib.mhd3d_closure_features.argtypes = [vp, vp, vp, vp, vp]
     lib.mhd3d_closure_loss.argtypes = [vp, vp, C.c_int64, vp, vp, vp]
@@ -345,6 +346,28 @@ class GpuSim:
         if st:
             raise Mhd3dError(st, "mhd3d_profiles")
         return out
+
+    def closure_set_bias(self, bias):
+        """Per-plane bias of the attached closure's tendencies, [7, NPZ]
+        float32 (RU, RV, RW, TT, BX, BY, BZ; host or device array); None
+        removes it."""
+        if bias is None:
+            st = self.lib.mhd3d_closure_set_bias(self.h, None)
+        else:
+            n = 7 * self.params.npz
+            if hasattr(bias, "data_ptr"):
+                bias = bias.float().contiguous()
+                if bias.numel() != n:
+                    raise ValueError(f"closure bias has {bias.numel()} values, expected {n}")
+                ptr = bias.data_ptr()
+            else:
+                bias = np.ascontiguousarray(bias, dtype=np.float32)
+                if bias.size != n:
+                    raise ValueError(f"closure bias has {bias.size} values, expected {n}")
+                ptr = bias.ctypes.data
+            st = self.lib.mhd3d_closure_set_bias(self.h, C.c_void_p(ptr))
+        if st:
+            raise Mhd3dError(st, "mhd3d_closure_set_bias")
 
     def closure_status(self) -> dict:
         t, e, r = C.c_int32(), C.c_int32(), C.c_int32()

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 ARGS = ["--fine", "64", "64", "32", "--ra", "1e5", "--ta", "1e4", "--contrast", "3", "--spin", "0.02",
         "--settle", "0.01", "--window", "0.06", "--samples", "3", "--chunk", "50", "--iters", "30",
-        "--resid-steps", "2", "--resid-iters", "30", "--gains", "1,0.5"]
+        "--resid-steps", "2", "--resid-iters", "30", "--gains", "1,0.5", "--bias"]
 
 
 def test_closure_case_small(mhd3d, tmp_path):
@@ -29,7 +29,8 @@ def test_closure_case_small(mhd3d, tmp_path):
     assert 0 < res["settle"] < 0.02   # the coarse runs start from the filtered state before the window
     assert res["train"]["pairs"] == 4 and res["train"]["residual"]["pairs"] == 4
     assert set(res["a_priori"]) == {"commutator_error_ratio", "residual_error_ratio", "commutator_vs_residual_ratio"}
-    assert res["train"]["gain_chosen"] in ("stress+heat+emf@1", "stress+heat+emf@0.5")
+    assert res["train"]["gain_chosen"] in ("stress+heat+emf@1", "stress+heat+emf@0.5", "stress+heat+emf@1|bias",
+                                           "stress+heat+emf@0.5|bias", "stress@0+heat@0+emf@0|bias")
     names = [k for k in res if k == "plain" or k.startswith("closure")]
     assert "plain" in names and len(names) >= 3   # plain, the default variant, the chosen gain
     for k in names:

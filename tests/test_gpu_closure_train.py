@@ -221,6 +221,48 @@ def test_closure_fallback_is_the_plain_step(mhd3d, npx):
     assert any(not np.array_equal(got2[f], ref[f]) for f in mhd3d.FIELDS)
 
 
+def test_closure_bias_is_a_per_plane_tendency(mhd3d):
+    """With the network's outputs scaled to zero, the closure's tendency is its
+    per-plane bias alone: a constant RU bias integrates to dt*b over one RK3
+    step on the interior planes (the coupling through the right-hand side is
+    second order in dt*b here), and a zero bias leaves the plain step."""
+    _gpu_or_skip(mhd3d)
+    torch = pytest.importorskip("torch")
+    import closure
+    setup = _coarse_setup(mhd3d, 64)
+    npz = setup.params.npz
+    plain = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    plain.upload(setup.state)
+    r0 = plain.step(1)
+    ref = plain.download()
+    net = closure.ClosureNet(seed=1)
+    net.out_scale = torch.zeros(12, device="cuda")
+    g = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    g.upload(setup.state)
+    net.attach(g, trip=1e30)
+    g.closure_set_bias(np.zeros((7, npz), dtype=np.float32))
+    g.step(1)
+    same = g.download()
+    for f in mhd3d.FIELDS:
+        assert np.array_equal(same[f], ref[f]), f
+    g.close()
+    b = 1e-3
+    bias = np.zeros((7, npz), dtype=np.float32)
+    bias[0, 1:-1] = b
+    h = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    h.upload(setup.state)
+    net.attach(h, trip=1e30)
+    h.closure_set_bias(torch.tensor(bias, device="cuda"))
+    h.step(1)
+    got = h.download()
+    assert h.closure_status()["trips"] == 0
+    d = (got["ru"] - ref["ru"])[1:-1, 1:-1, 4:-4] / (r0["dt"] * b)
+    assert np.abs(d - 1.0).max() < 0.05, np.abs(d - 1.0).max()
+    h.closure_set_bias(None)
+    h.close()
+    plain.close()
+
+
 def test_trained_network_gains_over_no_closure(mhd3d):
     """A priori: on held-out snapshots the trained closure's subgrid tendencies
     are closer to the filtered fine run's than no closure (zero) is."""
