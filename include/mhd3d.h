@@ -358,15 +358,18 @@ int mhd3d_closure_set(void* handle, const void* w1, const float* b1, const void*
                       const float* b3, const float* in_scale, const float* out_scale, float trip);
 int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* err);
 /*
- * A per-plane bias the attached closure adds to its tendencies (no
- * counterpart in the reference): bias[f*NPZ + k] for the fields RU, RV, RW,
- * TT, BX, BY, BZ (f = 0..6) and the interior planes k = 0..NPZ-1 (zero on
- * the walls, which take no tendency), a host or device array of 7*NPZ
- * floats, copied.  It is applied only on steps where the closure is (a step
- * that falls back to the plain coarse method takes neither).  Meant for the
- * horizontally uniform part of the coarse scheme's residual: the mismatch
- * between a box-filtered state and the coarse grid's own discrete balance.
- * NULL removes it.  FP32 handles only.
+ * A per-plane bias tendency of the closure (no counterpart in the
+ * reference): bias[f*NPZ + k] for the fields RU, RV, RW, TT, BX, BY, BZ
+ * (f = 0..6) and the interior planes k = 0..NPZ-1 (zero on the walls, which
+ * take no tendency), a host or device array of 7*NPZ floats, copied.  With a
+ * network attached it is added to the network's tendencies on every step
+ * that does not fall back to the plain coarse method (a step that falls back
+ * takes neither).  Without one, every step adds the bias alone: it is
+ * broadcast once into a tendency array of 7 floats per cell that the stage
+ * kernel reads, with no per-step evaluation.  Meant for the horizontally
+ * uniform part of the coarse scheme's residual: the mismatch between a
+ * box-filtered state and the coarse grid's own discrete balance.  NULL
+ * removes it.  FP32 handles only.
  */
 int mhd3d_closure_set_bias(void* handle, const float* bias);
 int mhd3d_coarsen(void* fine, int32_t fac, double* cstate, float* targets, void* stream);

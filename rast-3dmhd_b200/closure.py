@@ -164,6 +164,11 @@ class ClosureNet:
                                         C.c_float(trip))
         _check(st, "mhd3d_closure_set")
 
+    def detach(self, sim: mhd3d.GpuSim):
+        """Take the network off sim (a per-plane bias, if set, stays)."""
+        _check(self.lib.mhd3d_closure_set(sim.h, None, None, None, None, None, None, None, None, C.c_float(0.0)),
+               "mhd3d_closure_set")
+
 
 class PairCollector:
     """Coarse features and subgrid targets from snapshots of a fine run."""

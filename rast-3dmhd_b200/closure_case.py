@@ -276,10 +276,11 @@ def residual_bias(resid):
     return torch.stack([R.double().mean(dim=(2, 3)) for R, _ in resid]).mean(dim=0).float().contiguous()
 
 
-def a_priori(net, heldout, log):
+def a_priori(net, heldout, log, bias=None):
     """Tendency error ratio |pred - true|^2 / |true|^2 on the held-out run's
     last pair, whose filtered state is resident in the collector's coarse
-    handle (no closure gives 1)."""
+    handle (no closure gives 1); with a per-plane bias, also the residual
+    error ratios of the bias alone and of the network plus the bias."""
     torch = _torch()
     pc = heldout["pc"]
     s = torch.cuda.current_stream().cuda_stream
@@ -306,6 +307,10 @@ def a_priori(net, heldout, log):
         den = (wv * R ** 2).sum().item()
         out["residual_error_ratio"] = (wv * (pred_t - R) ** 2).sum().item() / den
         out["commutator_vs_residual_ratio"] = (wv * (true_t - R) ** 2).sum().item() / den
+        if bias is not None:
+            bv = bias.view(7, -1, 1, 1)
+            out["bias_residual_error_ratio"] = (wv * (bv - R) ** 2).sum().item() / den
+            out["network_and_bias_residual_error_ratio"] = (wv * (pred_t + bv - R) ** 2).sum().item() / den
         log(f"a priori residual error ratio {out['residual_error_ratio']:.4f} "
             f"(exact commutator: {out['commutator_vs_residual_ratio']:.4f})")
     return out
@@ -385,15 +390,20 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
         terms = terms[:-len("|bias")]
     else:
         bias = None
+    bias_only = False
     if net is not None:
         gains = term_gains(terms)
-        keep = net.out_scale
-        sc = net.out_scale.clone()
-        for name, idx in TERMS.items():
-            sc[list(idx)] *= gains.get(name, 0.0)
-        net.out_scale = sc
-        net.attach(g, trip=args.trip)
-        net.out_scale = keep
+        # with every gain zero the network adds nothing: the bias stands alone
+        # and no network is evaluated
+        bias_only = bias is not None and not any(gains.get(name, 0.0) for name in TERMS)
+        if not bias_only:
+            keep = net.out_scale
+            sc = net.out_scale.clone()
+            for name, idx in TERMS.items():
+                sc[list(idx)] *= gains.get(name, 0.0)
+            net.out_scale = sc
+            net.attach(g, trip=args.trip)
+            net.out_scale = keep
         if bias is not None:
             g.closure_set_bias(bias)
     profs = [g.profiles()]
@@ -431,7 +441,7 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
     out = {"status": status, "t_reached": t_end, "steps": steps, "wall_s": wall,
            "dt_mean": float(np.mean(dts)) if dts else None, "samples": len(profs)}
     if net is not None:
-        out["closure"] = g.closure_status()
+        out["closure"] = dict(g.closure_status(), bias_only=bias_only)
     out["profiles"] = np.mean(profs, axis=0)
     out["profiles_t"] = np.array(profs)
     g.close()
@@ -560,7 +570,7 @@ def main(argv=None):
         del trainer, data
         heldout = fine_phase(args, args.heldout_seed, False, log)
         heldout["resid_w"] = w
-        apri = a_priori(net, heldout, log)
+        apri = a_priori(net, heldout, log, bias if args.bias else None)
         if args.save:
             save_case(args.save, net, heldout, tr, apri, val, bias)
     chosen, chosen_eddy = None, (1.0, 1.0, 1.0)

@@ -65,6 +65,8 @@ struct Handle {
     __nv_bfloat16 *cfeat = nullptr, *cact1 = nullptr, *cact2 = nullptr;
     float *cpred = nullptr, *cfcl = nullptr;
     float* cbias = nullptr;   // closure: per-plane bias tendency [7][NPZ] (null: none)
+    float* cbtend = nullptr;  // that bias broadcast into the Z layout (7 fields), then a zero flag: the
+                              // tendencies a step adds when no network is attached
     double* cmeans = nullptr;                  // 3 x NPZ horizontal means (T, RO, BY)
     double* hpart = nullptr;                   // 3 x NPZ x HM_SPLIT partial sums of those means
     int* cflag = nullptr;                      // [0] trip flag of the current evaluation, [1] trips, [2] evaluations, [3] kernel error
@@ -669,6 +671,22 @@ __global__ void __launch_bounds__(TTX * TTY) k_tendency(UView v, const float* __
     }
 }
 
+// The per-plane bias alone, broadcast into the Z layout of the closure's
+// tendencies (zero on the wall planes, as k_tendency writes them).
+__global__ void __launch_bounds__(256) k_bias_tendency(const float* __restrict__ bias, int npx, int npy, int npz,
+                                                       float* __restrict__ out, size_t fstride, size_t kstride,
+                                                       size_t jstride)
+{
+    const size_t n = (size_t)npx * npy * npz;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % npx), j = (int)((c / npx) % npy), k = (int)(c / ((size_t)npx * npy));
+        float* o = out + (size_t)k * kstride + (size_t)j * jstride + i;
+        const bool wall = k == 0 || k == npz - 1;
+#pragma unroll
+        for (int f = 0; f < 7; ++f) o[f * fstride] = wall ? 0.f : bias[(size_t)f * npz + k];
+    }
+}
+
 cudaError_t launch_tendency(UView v, const float* pred, const float* osc, const Metrics& m, const float* bias, int npx,
                             int npy, int npz, float trip, float* out, size_t fstride, size_t kstride, size_t jstride,
                             int* flag, cudaStream_t st)
@@ -880,8 +898,8 @@ StageArgs32 make_args32(Handle* h)
     a.cx = h->cxy;
     a.cy = h->cxy + (h->p.npx + 2);
     a.s32 = h->s32;
-    a.fcl = h->clo ? h->cfcl : nullptr;
-    a.fcl_flag = h->cflag;
+    a.fcl = h->clo ? h->cfcl : h->cbtend;
+    a.fcl_flag = h->clo ? h->cflag : (h->cbtend ? reinterpret_cast<const int*>(h->cbtend + 7 * h->zf) : nullptr);
     a.top_lin = h->top_lin;
     a.top_tb = h->top_tb;
     a.t_top_fix = h->t_top_fix;
@@ -975,6 +993,7 @@ int destroy(Handle* h)
     cudaFree(h->cxy);
     cudaFree(h->cbuf);
     cudaFree(h->cbias);
+    cudaFree(h->cbtend);
     cudaFree(h->ctl);
     cudaFree(h->acc);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -2227,12 +2246,20 @@ int mhd3d_closure_set_bias(void* handle, const float* bias)
     if (int st = settle(h)) return st;
     if (!bias) {
         cudaFree(h->cbias);
-        h->cbias = nullptr;
+        cudaFree(h->cbtend);
+        h->cbias = h->cbtend = nullptr;
         return MHD3D_OK;
     }
-    const size_t n = (size_t)7 * h->p.npz;
+    const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
+    const size_t n = (size_t)7 * npz;
     if (!h->cbias) CK(cudaMalloc(&h->cbias, n * sizeof(float)));
     CK(cudaMemcpyAsync(h->cbias, bias, n * sizeof(float), cudaMemcpyDefault, h->st));
+    // for steps without a network: the tendencies once, and a zero trip flag
+    if (!h->cbtend) CK(cudaMalloc(&h->cbtend, 7 * h->zf * sizeof(float) + 4 * sizeof(int)));
+    CK(cudaMemsetAsync(h->cbtend + 7 * h->zf, 0, 4 * sizeof(int), h->st));
+    k_bias_tendency<<<grid_for((size_t)npx * npy * npz), 256, 0, h->st>>>(h->cbias, npx, npy, npz, h->cbtend, h->zf,
+                                                                          h->zz, (size_t)h->zpitch);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
     return MHD3D_OK;
 }

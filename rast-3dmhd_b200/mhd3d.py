@@ -348,9 +348,10 @@ class GpuSim:
         return out
 
     def closure_set_bias(self, bias):
-        """Per-plane bias of the attached closure's tendencies, [7, NPZ]
-        float32 (RU, RV, RW, TT, BX, BY, BZ; host or device array); None
-        removes it."""
+        """Per-plane bias tendency of the closure, [7, NPZ] float32 (RU, RV,
+        RW, TT, BX, BY, BZ; host or device array): added to an attached
+        network's tendencies, or applied alone on every step when no network
+        is attached; None removes it."""
         if bias is None:
             st = self.lib.mhd3d_closure_set_bias(self.h, None)
         else:

@@ -28,7 +28,8 @@ def test_closure_case_small(mhd3d, tmp_path):
     assert res["window"][1] > res["window"][0]
     assert 0 < res["settle"] < 0.02   # the coarse runs start from the filtered state before the window
     assert res["train"]["pairs"] == 4 and res["train"]["residual"]["pairs"] == 4
-    assert set(res["a_priori"]) == {"commutator_error_ratio", "residual_error_ratio", "commutator_vs_residual_ratio"}
+    assert set(res["a_priori"]) == {"commutator_error_ratio", "residual_error_ratio", "commutator_vs_residual_ratio",
+                                    "bias_residual_error_ratio", "network_and_bias_residual_error_ratio"}
     assert res["train"]["gain_chosen"] in ("stress+heat+emf@1", "stress+heat+emf@0.5", "stress+heat+emf@1|bias",
                                            "stress+heat+emf@0.5|bias", "stress@0+heat@0+emf@0|bias")
     names = [k for k in res if k == "plain" or k.startswith("closure")]
@@ -38,7 +39,9 @@ def test_closure_case_small(mhd3d, tmp_path):
         assert run["status"] == 0, (k, run)
         assert all(math.isfinite(v) for v in run["profile_rel_err"].values()), (k, run)
         if k != "plain":
-            assert run["closure"]["evals"] == run["steps"] and run["closure"]["err"] == 0
+            # the bias alone evaluates no network
+            evals = 0 if run["closure"]["bias_only"] else run["steps"]
+            assert run["closure"]["evals"] == evals and run["closure"]["err"] == 0
     # the reloaded case starts the coarse runs from the same filtered state
     again = closure_case.main(ARGS + ["--load", saved, "--variants", ""])
     assert again["plain"]["profile_rel_err"] == res["plain"]["profile_rel_err"]

@@ -258,6 +258,29 @@ def test_closure_bias_is_a_per_plane_tendency(mhd3d):
     assert h.closure_status()["trips"] == 0
     d = (got["ru"] - ref["ru"])[1:-1, 1:-1, 4:-4] / (r0["dt"] * b)
     assert np.abs(d - 1.0).max() < 0.05, np.abs(d - 1.0).max()
+    # without a network the bias stands alone: the same step, no evaluation
+    e = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    e.upload(setup.state)
+    e.closure_set_bias(bias)
+    e.step(1)
+    alone = e.download()
+    for f in mhd3d.FIELDS:
+        assert np.array_equal(alone[f], got[f]), f
+    assert e.closure_status()["evals"] == 0
+    # detaching the network from h leaves its bias alone as well
+    h.upload(setup.state)
+    net.detach(h)
+    h.step(1)
+    again = h.download()
+    for f in mhd3d.FIELDS:
+        assert np.array_equal(again[f], got[f]), f
+    e.closure_set_bias(None)
+    e.upload(setup.state)
+    e.step(1)
+    back = e.download()
+    for f in mhd3d.FIELDS:
+        assert np.array_equal(back[f], ref[f]), f
+    e.close()
     h.closure_set_bias(None)
     h.close()
     plain.close()
