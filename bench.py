@@ -426,6 +426,28 @@ def closure_measure(args, rank, world, local, dt_fine=None):
     fine_cells = w["npx"] * w["npy"] * w["npz"]
     fine_equiv = fine_cells * (dt_coarse / dt_fine) * args.steps / (ms / 1e3) / 1e6
 
+    # the closure as a per-plane bias tendency alone (no network attached, so
+    # none is evaluated): same grid, physics and step count, its own handle
+    import numpy as np
+    bsim = mhd3d.GpuSim(setup, mode=mhd3d.MODE_FP32)
+    bsim.set_stream(stream.cuda_stream)
+    bsim.upload(setup.state)
+    bias = np.zeros((7, setup.params.npz), dtype=np.float32)
+    bias[:, 1:-1] = 1e-6   # values do not change the cost
+    bsim.closure_set_bias(bias)
+    bsim.step(args.warmup)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    bsim.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    bms = e0.elapsed_time(e1)
+    bres = bsim.sync()
+    bsim.close()
+    bias_only = {"value": world * cells * args.steps / (bms / 1e3) / 1e6, "ms_per_step": bms / args.steps,
+                 "dt_coarse": bres["dt"], "status": bres["status"],
+                 "fine_equivalent_value": fine_cells * (bres["dt"] / dt_fine) * args.steps / (bms / 1e3) / 1e6}
+
     # tensor roofline of the convolutions: the three layers of one evaluation,
     # timed alone (CUDA events on the launching stream), against the burst
     # BF16 peak; algorithmic FLOPs 2*27*(8*32 + 32*32 + 32*12) per voxel (the
@@ -472,7 +494,7 @@ def closure_measure(args, rank, world, local, dt_fine=None):
             else "fallback 1.59 PFLOP/s"}
     return {"sim": sim, "setup": setup, "cfg": cfg, "stream": stream, "cells": cells, "ms": ms, "value": value,
             "status": status, "dt_coarse": dt_coarse, "dt_fine": dt_fine, "fine_equiv": fine_equiv, "roof": roof,
-            "clocks": clk}
+            "clocks": clk, "bias_only": bias_only}
 
 
 def closure_profile_record():
@@ -499,6 +521,8 @@ def closure_summary(args, rank, world, local, dt_fine):
             "fine_equivalent_value": cm["fine_equiv"],
             "fine_equivalent_formula": "512^2*256 cells x (DT_coarse/DT_fine) x steps / coarse wall",
             "closure_status": cm["status"], "conv_roofline": cm["roof"],
+            "bias_only": dict(cm["bias_only"], workload="the same coarse run with the closure's per-plane bias "
+                              "tendency alone (no network attached), the closure chosen in the recorded case"),
             "profile_error": closure_profile_record()}
 
 
