@@ -350,6 +350,25 @@ def gain_grid(spec):
     return cands
 
 
+def with_bias(cands):
+    """Every candidate terms string again with the per-plane bias ("|bias"),
+    and the bias alone (every group at gain 0), without repeats."""
+    zero = "+".join(f"{g}@0" for g in TERMS)
+    return list(dict.fromkeys(cands + [c + "|bias" for c in cands] + [zero + "|bias"]))
+
+
+def split_bias(terms):
+    """(terms without a trailing "|bias", whether it had one)."""
+    return (terms[:-len("|bias")], True) if terms.endswith("|bias") else (terms, False)
+
+
+def bias_alone(terms, has_bias):
+    """True when every term group's gain is zero and a bias is applied: the
+    network adds nothing, so the coarse run attaches none."""
+    gains = term_gains(terms)
+    return has_bias and not any(gains.get(name, 0.0) for name in TERMS)
+
+
 def eddy_factors(spec):
     """Candidate (viscosity, conduction, magnetic diffusivity) factors of
     "1,1.5:1.5:1,2": a bare number scales all three."""
@@ -386,16 +405,15 @@ def coarse_phase(heldout, net, args, log, tag, terms="stress+heat+emf", eddy=(1.
     diffusion coefficients (eddy_setup)."""
     g = mhd3d.GpuSim(eddy_setup(heldout["coarse_setup"], eddy), mode=mhd3d.MODE_FP32)
     g.upload(heldout["start"])
-    if terms.endswith("|bias"):
-        terms = terms[:-len("|bias")]
-    else:
+    terms, use_bias = split_bias(terms)
+    if not use_bias:
         bias = None
     bias_only = False
     if net is not None:
         gains = term_gains(terms)
         # with every gain zero the network adds nothing: the bias stands alone
         # and no network is evaluated
-        bias_only = bias is not None and not any(gains.get(name, 0.0) for name in TERMS)
+        bias_only = bias_alone(terms, bias is not None)
         if not bias_only:
             keep = net.out_scale
             sc = net.out_scale.clone()
@@ -577,9 +595,7 @@ def main(argv=None):
     cands = gain_grid(args.gain_grid) if args.gain_grid else (
         [f"{args.gain_terms}@{gv}" for gv in args.gains.split(",")] if args.gains else [])
     if args.bias and bias is not None and cands:
-        # every candidate again with the per-plane bias, and the bias alone
-        zero = "+".join(f"{g}@0" for g in TERMS)
-        cands = list(dict.fromkeys(cands + [c + "|bias" for c in cands] + [zero + "|bias"]))
+        cands = with_bias(cands)
     eddies = eddy_factors(args.eddy)
     if (cands or len(eddies) > 1) and val is not None:
         # gains and eddy factors are chosen on the training run's own window, never on the held-out run's

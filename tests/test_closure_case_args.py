@@ -41,3 +41,31 @@ def test_eddy_setup_scales_the_diffusion_coefficients():
     assert q.orm == p.orm * 3.0 and q.rm == p.rm / 3.0
     assert q.npx == p.npx and q.ocv == p.ocv and q.grav == p.grav
     assert e.grid is su.grid and e.state is su.state
+
+
+def test_bias_candidates():
+    c = closure_case.with_bias(closure_case.gain_grid("stress+heat:0,0.25;emf:0"))
+    assert c == ["stress@0+heat@0+emf@0", "stress@0.25+heat@0.25+emf@0",
+                 "stress@0+heat@0+emf@0|bias", "stress@0.25+heat@0.25+emf@0|bias"]   # the bias alone once
+    assert closure_case.with_bias(["stress+heat+emf@0.5"])[-1] == "stress@0+heat@0+emf@0|bias"
+    assert closure_case.split_bias("stress@0.06+heat@0.06+emf@0.12|bias") == ("stress@0.06+heat@0.06+emf@0.12", True)
+    assert closure_case.split_bias("stress+heat+emf@0.12") == ("stress+heat+emf@0.12", False)
+    assert closure_case.bias_alone("stress@0+heat@0+emf@0", True)
+    assert not closure_case.bias_alone("stress@0+heat@0+emf@0", False)
+    assert not closure_case.bias_alone("stress@0+heat@0+emf@0.12", True)
+    assert closure_case.bias_alone("emf@0", True)   # groups not named take no network term
+
+
+def test_residual_bias_is_the_mean_horizontal_profile():
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(3)
+    nz, ny, nx = 6, 5, 8
+    prof = torch.randn(7, nz, 1, 1, generator=g, dtype=torch.float64)
+    pairs = []
+    for s in (1.0, 3.0):
+        noise = torch.randn(7, nz, ny, nx, generator=g, dtype=torch.float64)
+        noise -= noise.mean(dim=(2, 3), keepdim=True)
+        pairs.append(((s * prof + noise).float(), None))
+    b = closure_case.residual_bias(pairs)
+    assert b.shape == (7, nz) and b.dtype == torch.float32
+    assert torch.allclose(b.double(), 2.0 * prof[:, :, 0, 0], rtol=1e-5, atol=1e-6)
