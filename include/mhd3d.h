@@ -369,7 +369,8 @@ int mhd3d_closure_status(void* handle, int32_t* trips, int32_t* evals, int32_t* 
  * kernel reads, with no per-step evaluation.  Meant for the horizontally
  * uniform part of the coarse scheme's residual: the mismatch between a
  * box-filtered state and the coarse grid's own discrete balance.  NULL
- * removes it.  FP32 handles only.
+ * removes it; a call that fails leaves the handle without a bias.  FP32
+ * handles only.
  */
 int mhd3d_closure_set_bias(void* handle, const float* bias);
 int mhd3d_coarsen(void* fine, int32_t fac, double* cstate, float* targets, void* stream);

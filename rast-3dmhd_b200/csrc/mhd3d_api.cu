@@ -2252,15 +2252,38 @@ int mhd3d_closure_set_bias(void* handle, const float* bias)
     }
     const int npx = h->p.npx, npy = h->p.npy, npz = h->p.npz;
     const size_t n = (size_t)7 * npz;
-    if (!h->cbias) CK(cudaMalloc(&h->cbias, n * sizeof(float)));
-    CK(cudaMemcpyAsync(h->cbias, bias, n * sizeof(float), cudaMemcpyDefault, h->st));
-    // for steps without a network: the tendencies once, and a zero trip flag
-    if (!h->cbtend) CK(cudaMalloc(&h->cbtend, 7 * h->zf * sizeof(float) + 4 * sizeof(int)));
-    CK(cudaMemsetAsync(h->cbtend + 7 * h->zf, 0, 4 * sizeof(int), h->st));
-    k_bias_tendency<<<grid_for((size_t)npx * npy * npz), 256, 0, h->st>>>(h->cbias, npx, npy, npz, h->cbtend, h->zf,
-                                                                          h->zz, (size_t)h->zpitch);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(h->st));
+    // the bias and, for steps without a network, its tendencies and a zero
+    // trip flag: both buffers or neither
+    if (!h->cbias || !h->cbtend) {
+        cudaFree(h->cbias);
+        cudaFree(h->cbtend);
+        h->cbias = h->cbtend = nullptr;
+        float *pb = nullptr, *pt = nullptr;
+        if (cudaMalloc(&pb, n * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&pt, 7 * h->zf * sizeof(float) + 4 * sizeof(int)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            cudaFree(pb);
+            return MHD3D_ERR_NOMEM;
+        }
+        h->cbias = pb;
+        h->cbtend = pt;
+    }
+    cudaError_t e = cudaMemcpyAsync(h->cbias, bias, n * sizeof(float), cudaMemcpyDefault, h->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->cbtend + 7 * h->zf, 0, 4 * sizeof(int), h->st);
+    if (e == cudaSuccess) {
+        k_bias_tendency<<<grid_for((size_t)npx * npy * npz), 256, 0, h->st>>>(h->cbias, npx, npy, npz, h->cbtend,
+                                                                              h->zf, h->zz, (size_t)h->zpitch);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) {
+        // no half-set bias: the handle is left without one
+        std::fprintf(stderr, "mhd3d: mhd3d_closure_set_bias failed: %s\n", cudaGetErrorString(e));
+        cudaFree(h->cbias);
+        cudaFree(h->cbtend);
+        h->cbias = h->cbtend = nullptr;
+        return MHD3D_ERR_CUDA;
+    }
     return MHD3D_OK;
 }
 

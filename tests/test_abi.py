@@ -49,6 +49,7 @@ def test_bad_arguments_rejected_before_device_use(mhd3d):
     assert lib.mhd3d_step(None, 1, None, None, None, None, None) == 1
     assert lib.mhd3d_upload(None, *([None] * 8)) == 1
     assert lib.mhd3d_destroy(None) == 0
+    assert lib.mhd3d_closure_set_bias(None, None) == 1
     # closure convolutions: empty extents, a channel pair that is not built, missing outputs
     buf = C.create_string_buffer(64)
     p = C.cast(buf, C.c_void_p)
