@@ -98,5 +98,24 @@ module mhd3d_gpu
        type(c_ptr), value :: ddx, ddy, ddz, rkapa
        type(c_ptr), value :: out, stream
      end function mhd3d_cfl_noalloc
+
+     ! Per-plane bias tendency of an FP32 coarse run's closure (no counterpart
+     ! in the reference driver): BIAS(K-1, F) for plane K=2..NZ-1 and field
+     ! F = RU, RV, RW, TT, BX, BY, BZ (1..7), an NPZ x 7 array; the wall
+     ! planes K=2 and K=NZ-1 take none.  Without a network attached every
+     ! step adds the bias alone.
+     integer(c_int) function mhd3d_closure_set_bias(handle, bias) bind(C, name="mhd3d_closure_set_bias")
+       import :: c_int, c_float, c_ptr
+       type(c_ptr), value :: handle
+       real(c_float), intent(in) :: bias(*)
+     end function mhd3d_closure_set_bias
+
+     ! steps that fell back to the plain coarse method, network evaluations,
+     ! and the closure kernels' error flag
+     integer(c_int) function mhd3d_closure_status(handle, trips, evals, err) bind(C, name="mhd3d_closure_status")
+       import :: c_int, c_int32_t, c_ptr
+       type(c_ptr), value :: handle
+       integer(c_int32_t), intent(out) :: trips, evals, err
+     end function mhd3d_closure_status
   end interface
 end module mhd3d_gpu
